@@ -1,0 +1,475 @@
+// Host orchestration of the MSM pipeline: planning, scratch layout, launch
+// sequence and the msm_* C ABI.  Mirrors the reference's msm::execute_async
+// (src/msm.cu:419-460) and schedule_execution (src/msm.cu:85-417): one call
+// enqueues the whole pipeline on the caller's stream, all temporaries come
+// from the caller's memory pool in stream order, and host-resident scalars,
+// bases and results are copied in / out with the optional events and
+// callbacks fired after the copies.
+#include "bellman-cuda.h"
+#include "bellman-cuda-b200.h"
+#include "msm_host.cuh"
+#include "msm_kernels.cuh"
+
+#include <algorithm>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+namespace msm_b200 {
+
+#define CHECK(statement)                                                                                                                       \
+  do {                                                                                                                                         \
+    cudaError_t check_result_ = (statement);                                                                                                   \
+    if (check_result_ != cudaSuccess)                                                                                                          \
+      return check_result_;                                                                                                                    \
+  } while (0)
+
+static unsigned ceil_log2(unsigned long long v) {
+  unsigned r = 0;
+  while ((1ull << r) < v)
+    r++;
+  return r;
+}
+
+// Window width by problem size: Pippenger cost ~ (n + 1.4 * 2^c) / c point
+// additions, minimised near c = log2(n) - 3 .. - 6 at the sizes of interest;
+// capped at 16 so keys need at most two 8-bit sort passes.
+unsigned default_window_bits(unsigned long long n) {
+  const unsigned lg = ceil_log2(n);
+  if (lg <= 6)
+    return 3;
+  if (lg <= 20)
+    return std::max(3u, lg - 4);
+  return 16;
+}
+
+struct device_info {
+  int sms = 0;
+};
+
+static device_info get_device_info(int device) {
+  static std::mutex lock;
+  static device_info cache[64];
+  std::lock_guard<std::mutex> guard(lock);
+  if (device < 0 || device >= 64)
+    return device_info{148};
+  if (cache[device].sms == 0) {
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || sms <= 0)
+      sms = 148;
+    cache[device].sms = sms;
+  }
+  return cache[device];
+}
+
+plan make_plan(unsigned n, unsigned window_bits, int sms) {
+  plan p{};
+  p.n = n;
+  p.c = window_bits ? window_bits : default_window_bits(n);
+  p.windows = (RESULT_BITS + p.c - 1) / p.c;
+  p.log_b = p.c - 1;
+  p.key_bits = p.c; // keys are |d| in [0, 2^(c-1)]
+  p.sort_passes = (p.key_bits + SORT_RADIX_BITS - 1) / SORT_RADIX_BITS;
+  p.tiles = (n + SORT_TILE - 1) / SORT_TILE;
+  // One accumulation range per resident thread (4 blocks of ACC_THREADS per
+  // SM), fewer for small inputs so that every range has work.
+  const unsigned long long entries = (unsigned long long)p.windows * n;
+  const unsigned long long full = (unsigned long long)sms * 4 * ACC_THREADS;
+  p.acc_threads = (unsigned)std::max(1ull, std::min(full, (entries + 7) / 8));
+  p.merge_chunk = 4;
+  p.log_m = std::min(4u, p.log_b);
+  p.log_g = p.log_b - p.log_m;
+  p.groups = 1u << p.log_g;
+  p.sum_fanin = 8;
+  return p;
+}
+
+// Scratch layout inside one pool allocation.
+struct layout {
+  size_t keys[2], vals[2], counts, zeros, buckets, flags, hb[2], hp[2], tree[2], streams[2], results, scalars, bases, total;
+};
+
+static size_t align_up(size_t v) { return (v + 255) & ~(size_t)255; }
+
+static layout make_layout(const plan &p, bool copy_scalars, bool copy_bases, bool copy_results) {
+  layout l{};
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    const size_t at = off;
+    off += align_up(bytes);
+    return at;
+  };
+  const size_t entries = (size_t)p.windows * p.n;
+  for (int i = 0; i < 2; i++) {
+    l.keys[i] = take(entries * 4);
+    l.vals[i] = take(entries * 4);
+  }
+  l.counts = take((size_t)p.windows * SORT_RADIX * p.tiles * 4);
+  l.zeros = take((size_t)p.windows * 4);
+  const size_t slots = (size_t)p.windows << p.log_b;
+  l.buckets = take(slots * sizeof(xyzz));
+  l.flags = take(slots);
+  for (int i = 0; i < 2; i++) {
+    l.hb[i] = take((size_t)p.acc_threads * 4);
+    l.hp[i] = take((size_t)p.acc_threads * sizeof(xyzz));
+  }
+  for (int i = 0; i < 2; i++) {
+    l.tree[i] = take(((size_t)p.windows << p.log_g) * sizeof(xyzz));
+    l.streams[i] = take((size_t)p.windows * stream_stride(p.log_g) * sizeof(xyzz));
+  }
+  l.results = copy_results ? take(RESULT_BITS * sizeof(jacobian)) : 0;
+  l.scalars = copy_scalars ? take((size_t)p.n * sizeof(fe)) : 0;
+  l.bases = copy_bases ? take((size_t)p.n * sizeof(affine)) : 0;
+  l.total = off;
+  return l;
+}
+
+size_t scratch_bytes(unsigned n, unsigned window_bits, bool copy_scalars, bool copy_bases, bool copy_results) {
+  int device = 0;
+  cudaGetDevice(&device);
+  const plan p = make_plan(n, window_bits, get_device_info(device).sms);
+  return make_layout(p, copy_scalars, copy_bases, copy_results).total;
+}
+
+static bool is_host_pointer(const void *ptr, cudaError_t &err) {
+  cudaPointerAttributes attr{};
+  err = cudaPointerGetAttributes(&attr, ptr);
+  if (err != cudaSuccess)
+    return false;
+  return attr.type == cudaMemoryTypeUnregistered || attr.type == cudaMemoryTypeHost;
+}
+
+// Enqueue the kernels of one MSM whose inputs are on the device.
+// stage_events (optional): PROFILE_STAGES + 1 events recorded before the first
+// stage and after each stage.  launches (optional): kernels enqueued.
+cudaError_t enqueue_pipeline(const plan &p, const fe *scalars, const affine *bases, jacobian *results, uint8_t *scratch, const layout &l,
+                             cudaStream_t stream, cudaEvent_t *stage_events = nullptr, unsigned *launches = nullptr) {
+  unsigned launched = 0;
+  unsigned stage = 0;
+  auto mark = [&]() -> cudaError_t { return stage_events ? cudaEventRecord(stage_events[stage++], stream) : cudaSuccess; };
+  CHECK(mark());
+  uint32_t *keys[2] = {reinterpret_cast<uint32_t *>(scratch + l.keys[0]), reinterpret_cast<uint32_t *>(scratch + l.keys[1])};
+  uint32_t *vals[2] = {reinterpret_cast<uint32_t *>(scratch + l.vals[0]), reinterpret_cast<uint32_t *>(scratch + l.vals[1])};
+  uint32_t *counts = reinterpret_cast<uint32_t *>(scratch + l.counts);
+  uint32_t *zeros = reinterpret_cast<uint32_t *>(scratch + l.zeros);
+  xyzz *buckets = reinterpret_cast<xyzz *>(scratch + l.buckets);
+  uint8_t *flags = scratch + l.flags;
+  uint32_t *hb[2] = {reinterpret_cast<uint32_t *>(scratch + l.hb[0]), reinterpret_cast<uint32_t *>(scratch + l.hb[1])};
+  xyzz *hp[2] = {reinterpret_cast<xyzz *>(scratch + l.hp[0]), reinterpret_cast<xyzz *>(scratch + l.hp[1])};
+  xyzz *tree[2] = {reinterpret_cast<xyzz *>(scratch + l.tree[0]), reinterpret_cast<xyzz *>(scratch + l.tree[1])};
+  xyzz *streams[2] = {reinterpret_cast<xyzz *>(scratch + l.streams[0]), reinterpret_cast<xyzz *>(scratch + l.streams[1])};
+  const unsigned n = p.n;
+
+  // 1. digits
+  digits_kernel<<<(n + 255) / 256, 256, 0, stream>>>(scalars, n, p.c, p.windows, keys[0], vals[0]);
+  CHECK(cudaGetLastError());
+  launched++;
+  CHECK(mark());
+
+  // 2. sort, 8 bits per pass
+  int cur = 0;
+  for (unsigned pass = 0; pass < p.sort_passes; pass++) {
+    const unsigned shift = pass * SORT_RADIX_BITS;
+    const dim3 grid(p.tiles, p.windows);
+    sort_histogram_kernel<<<grid, SORT_THREADS, 0, stream>>>(keys[cur], n, p.tiles, shift, counts);
+    CHECK(cudaGetLastError());
+    sort_scan_kernel<<<p.windows, 1024, 0, stream>>>(counts, p.tiles);
+    CHECK(cudaGetLastError());
+    sort_scatter_kernel<<<grid, SORT_THREADS, 0, stream>>>(keys[cur], vals[cur], keys[cur ^ 1], vals[cur ^ 1], n, p.tiles, shift, counts);
+    CHECK(cudaGetLastError());
+    launched += 3;
+    cur ^= 1;
+  }
+  CHECK(mark());
+
+  // 3. zero-digit prefix of every window
+  zero_counts_kernel<<<(p.windows + 127) / 128, 128, 0, stream>>>(keys[cur], n, p.windows, zeros);
+  CHECK(cudaGetLastError());
+  launched++;
+  CHECK(cudaMemsetAsync(flags, 0, (size_t)p.windows << p.log_b, stream));
+  CHECK(mark());
+
+  // 4. accumulation
+  accumulate_kernel<<<(p.acc_threads + ACC_THREADS - 1) / ACC_THREADS, ACC_THREADS, 0, stream>>>(
+      keys[cur], vals[cur], bases, n, p.windows, p.log_b, zeros, p.acc_threads, buckets, flags, hb[0], hp[0]);
+  CHECK(cudaGetLastError());
+  launched++;
+  CHECK(mark());
+
+  // 5. heads
+  unsigned heads = p.acc_threads;
+  int h = 0;
+  while (heads > 1) {
+    const unsigned out = (heads + p.merge_chunk - 1) / p.merge_chunk;
+    merge_heads_kernel<<<(out + ACC_THREADS - 1) / ACC_THREADS, ACC_THREADS, 0, stream>>>(hb[h], hp[h], heads, p.merge_chunk, buckets,
+                                                                                           hb[h ^ 1], hp[h ^ 1]);
+    CHECK(cudaGetLastError());
+    launched++;
+    heads = out;
+    h ^= 1;
+  }
+  CHECK(mark());
+
+  // 6. reduction
+  const unsigned group_threads = p.windows << p.log_g;
+  reduce_groups_kernel<<<(group_threads + ACC_THREADS - 1) / ACC_THREADS, ACC_THREADS, 0, stream>>>(buckets, flags, p.windows, p.log_b,
+                                                                                                     p.log_m, tree[0], streams[0]);
+  CHECK(cudaGetLastError());
+  launched++;
+  int t = 0;
+  for (unsigned level = 0; level < p.log_g; level++) {
+    const unsigned threads = p.windows * ((1u << p.log_g) >> (level + 1));
+    reduce_tree_kernel<<<(threads + ACC_THREADS - 1) / ACC_THREADS, ACC_THREADS, 0, stream>>>(tree[t], tree[t ^ 1], streams[0], p.windows,
+                                                                                               p.log_g, level);
+    CHECK(cudaGetLastError());
+    launched++;
+    t ^= 1;
+  }
+  int s = 0;
+  unsigned divisor = 1;
+  while (divisor < p.groups) {
+    const unsigned len_out = ((p.groups + divisor - 1) / divisor + p.sum_fanin - 1) / p.sum_fanin;
+    const dim3 grid((len_out + ACC_THREADS - 1) / ACC_THREADS, p.windows * (p.log_g + 1));
+    reduce_streams_kernel<<<grid, ACC_THREADS, 0, stream>>>(streams[s], streams[s ^ 1], p.windows, p.log_g, p.sum_fanin, divisor);
+    CHECK(cudaGetLastError());
+    launched++;
+    divisor *= p.sum_fanin;
+    s ^= 1;
+  }
+  gather_results_kernel<<<(RESULT_BITS + 127) / 128, 128, 0, stream>>>(streams[s], buckets, flags, p.windows, p.c, p.log_m, p.log_g,
+                                                                       divisor, results);
+  CHECK(cudaGetLastError());
+  launched++;
+  CHECK(mark());
+  if (launches)
+    *launches = launched;
+  return cudaSuccess;
+}
+
+// Synchronises the stream, then reads the stage times and the work counts
+// that the scratch buffers still hold.
+static cudaError_t collect_profile(const plan &p, const layout &l, const uint8_t *scratch, cudaStream_t stream, const cudaEvent_t *events,
+                                   unsigned launches, msm_b200_profile *out) {
+  CHECK(cudaStreamSynchronize(stream));
+  *out = msm_b200_profile{};
+  for (unsigned s = 0; s < PROFILE_STAGES; s++)
+    CHECK(cudaEventElapsedTime(&out->stage_ms[s], events[s], events[s + 1]));
+  std::vector<uint32_t> zeros(p.windows);
+  CHECK(cudaMemcpy(zeros.data(), scratch + l.zeros, zeros.size() * 4, cudaMemcpyDeviceToHost));
+  std::vector<uint8_t> flags((size_t)p.windows << p.log_b);
+  CHECK(cudaMemcpy(flags.data(), scratch + l.flags, flags.size(), cudaMemcpyDeviceToHost));
+  std::vector<uint32_t> heads(p.acc_threads);
+  CHECK(cudaMemcpy(heads.data(), scratch + l.hb[0], heads.size() * 4, cudaMemcpyDeviceToHost));
+  unsigned long long nonzero = 0, nonempty = 0, continued = 0;
+  for (uint32_t z : zeros)
+    nonzero += p.n - z;
+  for (uint8_t f : flags)
+    nonempty += f != 0;
+  for (uint32_t h : heads)
+    continued += h != INVALID_BUCKET;
+  out->nonzero_entries = nonzero;
+  out->nonempty_buckets = nonempty;
+  out->heads = continued;
+  out->window_bits = p.c;
+  out->windows = p.windows;
+  out->acc_threads = p.acc_threads;
+  out->launches = launches;
+  return cudaSuccess;
+}
+
+cudaError_t execute(const execution &e) {
+  if (e.count == 0 || e.count > (1u << 31) || !e.scalars || !e.bases || !e.results)
+    return cudaErrorInvalidValue;
+  if ((reinterpret_cast<uintptr_t>(e.bases) & 15) || (reinterpret_cast<uintptr_t>(e.scalars) & 15))
+    return cudaErrorInvalidValue;
+  if (e.window_bits && (e.window_bits < 2 || e.window_bits > 24))
+    return cudaErrorInvalidValue;
+  int device = 0;
+  CHECK(cudaGetDevice(&device));
+  cudaError_t err;
+  const bool copy_scalars = is_host_pointer(e.scalars, err);
+  CHECK(err);
+  const bool copy_bases = is_host_pointer(e.bases, err);
+  CHECK(err);
+  const bool copy_results = is_host_pointer(e.results, err);
+  CHECK(err);
+  const plan p = make_plan(e.count, e.window_bits, get_device_info(device).sms);
+  if (p.windows > 128)
+    return cudaErrorInvalidValue;
+  const layout l = make_layout(p, copy_scalars, copy_bases, copy_results);
+  cudaStream_t stream = e.stream;
+  void *raw = nullptr;
+  if (e.pool)
+    CHECK(cudaMallocFromPoolAsync(&raw, l.total, e.pool, stream));
+  else
+    CHECK(cudaMallocAsync(&raw, l.total, stream));
+  uint8_t *scratch = static_cast<uint8_t *>(raw);
+  cudaError_t status = cudaSuccess;
+  do {
+    const fe *scalars = static_cast<const fe *>(e.scalars);
+    const affine *bases = static_cast<const affine *>(e.bases);
+    jacobian *results = static_cast<jacobian *>(e.results);
+    if (copy_scalars) {
+      if ((status = cudaMemcpyAsync(scratch + l.scalars, e.scalars, (size_t)p.n * sizeof(fe), cudaMemcpyHostToDevice, stream)) != cudaSuccess)
+        break;
+      scalars = reinterpret_cast<const fe *>(scratch + l.scalars);
+    }
+    if (copy_bases) {
+      if ((status = cudaMemcpyAsync(scratch + l.bases, e.bases, (size_t)p.n * sizeof(affine), cudaMemcpyHostToDevice, stream)) != cudaSuccess)
+        break;
+      bases = reinterpret_cast<const affine *>(scratch + l.bases);
+    }
+    if (copy_scalars || copy_bases) {
+      if (e.h2d_event && (status = cudaEventRecord(e.h2d_event, stream)) != cudaSuccess)
+        break;
+      if (e.h2d_callback && (status = cudaLaunchHostFunc(stream, e.h2d_callback, e.h2d_callback_data)) != cudaSuccess)
+        break;
+    }
+    jacobian *device_results = copy_results ? reinterpret_cast<jacobian *>(scratch + l.results) : results;
+    cudaEvent_t events[PROFILE_STAGES + 1] = {};
+    const cudaEvent_t *stage_events = e.stage_events;
+    if (e.profile) {
+      for (auto &ev : events)
+        if ((status = cudaEventCreate(&ev)) != cudaSuccess)
+          break;
+      if (status != cudaSuccess)
+        break;
+    }
+    unsigned launches = 0;
+    if (e.profile)
+      stage_events = events;
+    if ((status = enqueue_pipeline(p, scalars, bases, device_results, scratch, l, stream, const_cast<cudaEvent_t *>(stage_events), &launches)) !=
+        cudaSuccess)
+      break;
+    if (e.launches)
+      *e.launches = launches;
+    if (e.profile) {
+      status = collect_profile(p, l, scratch, stream, events, launches, e.profile);
+      for (auto &ev : events)
+        cudaEventDestroy(ev);
+      if (status != cudaSuccess)
+        break;
+    }
+    if (copy_results) {
+      if ((status = cudaMemcpyAsync(e.results, device_results, RESULT_BITS * sizeof(jacobian), cudaMemcpyDeviceToHost, stream)) != cudaSuccess)
+        break;
+      if (e.d2h_event && (status = cudaEventRecord(e.d2h_event, stream)) != cudaSuccess)
+        break;
+      if (e.d2h_callback && (status = cudaLaunchHostFunc(stream, e.d2h_callback, e.d2h_callback_data)) != cudaSuccess)
+        break;
+    }
+  } while (false);
+  const cudaError_t free_status = cudaFreeAsync(raw, stream);
+  return status != cudaSuccess ? status : free_status;
+}
+
+template <class F> static cudaError_t set_l1_preference(F *func) {
+  CHECK(cudaFuncSetAttribute(func, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxL1));
+  return cudaSuccess;
+}
+
+cudaError_t set_up() {
+  CHECK(set_l1_preference(accumulate_kernel));
+  CHECK(set_l1_preference(merge_heads_kernel));
+  CHECK(set_l1_preference(reduce_groups_kernel));
+  CHECK(set_l1_preference(reduce_tree_kernel));
+  CHECK(set_l1_preference(reduce_streams_kernel));
+  CHECK(set_l1_preference(digits_kernel));
+  return cudaSuccess;
+}
+
+} // namespace msm_b200
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+bc_error msm_set_up() { return static_cast<bc_error>(msm_b200::set_up()); }
+
+bc_error msm_execute_async(const msm_configuration configuration) {
+  if (configuration.log_scalars_count > 31)
+    return bc_error_invalid_value;
+  msm_b200::execution e{};
+  e.pool = static_cast<cudaMemPool_t>(configuration.mem_pool.handle);
+  e.stream = static_cast<cudaStream_t>(configuration.stream.handle);
+  e.bases = configuration.bases;
+  e.scalars = configuration.scalars;
+  e.results = configuration.results;
+  e.count = 1u << configuration.log_scalars_count;
+  e.window_bits = 0;
+  e.h2d_event = static_cast<cudaEvent_t>(configuration.h2d_copy_finished.handle);
+  e.h2d_callback = configuration.h2d_copy_finished_callback;
+  e.h2d_callback_data = configuration.h2d_copy_finished_callback_data;
+  e.d2h_event = static_cast<cudaEvent_t>(configuration.d2h_copy_finished.handle);
+  e.d2h_callback = configuration.d2h_copy_finished_callback;
+  e.d2h_callback_data = configuration.d2h_copy_finished_callback_data;
+  return static_cast<bc_error>(msm_b200::execute(e));
+}
+
+bc_error msm_tear_down() { return bc_success; }
+
+bc_error msm_b200_execute_async(const msm_b200_configuration *configuration) {
+  if (!configuration)
+    return bc_error_invalid_value;
+  msm_b200::execution e{};
+  e.pool = static_cast<cudaMemPool_t>(configuration->mem_pool.handle);
+  e.stream = static_cast<cudaStream_t>(configuration->stream.handle);
+  e.bases = configuration->bases;
+  e.scalars = configuration->scalars;
+  e.results = configuration->results;
+  e.count = configuration->count;
+  e.window_bits = configuration->window_bits;
+  return static_cast<bc_error>(msm_b200::execute(e));
+}
+
+bc_error msm_b200_execute_profiled(const msm_b200_configuration *configuration, msm_b200_profile *profile) {
+  if (!configuration || !profile)
+    return bc_error_invalid_value;
+  msm_b200::execution e{};
+  e.pool = static_cast<cudaMemPool_t>(configuration->mem_pool.handle);
+  e.stream = static_cast<cudaStream_t>(configuration->stream.handle);
+  e.bases = configuration->bases;
+  e.scalars = configuration->scalars;
+  e.results = configuration->results;
+  e.count = configuration->count;
+  e.window_bits = configuration->window_bits;
+  e.profile = profile;
+  return static_cast<bc_error>(msm_b200::execute(e));
+}
+
+bc_error msm_b200_execute_staged_async(const msm_b200_configuration *configuration, const bc_event *stage_events, unsigned *launches) {
+  if (!configuration || !stage_events)
+    return bc_error_invalid_value;
+  cudaEvent_t events[msm_b200::PROFILE_STAGES + 1];
+  for (unsigned i = 0; i <= msm_b200::PROFILE_STAGES; i++)
+    events[i] = static_cast<cudaEvent_t>(stage_events[i].handle);
+  msm_b200::execution e{};
+  e.pool = static_cast<cudaMemPool_t>(configuration->mem_pool.handle);
+  e.stream = static_cast<cudaStream_t>(configuration->stream.handle);
+  e.bases = configuration->bases;
+  e.scalars = configuration->scalars;
+  e.results = configuration->results;
+  e.count = configuration->count;
+  e.window_bits = configuration->window_bits;
+  e.stage_events = events;
+  e.launches = launches;
+  return static_cast<bc_error>(msm_b200::execute(e));
+}
+
+bc_error msm_b200_scratch_bytes(unsigned count, unsigned window_bits, size_t *bytes) {
+  if (!bytes || count == 0)
+    return bc_error_invalid_value;
+  *bytes = msm_b200::scratch_bytes(count, window_bits, false, false, false);
+  return bc_success;
+}
+
+bc_error msm_b200_default_window_bits(unsigned count, unsigned *window_bits) {
+  if (!window_bits || count == 0)
+    return bc_error_invalid_value;
+  *window_bits = msm_b200::default_window_bits(count);
+  return bc_success;
+}
+
+} // extern "C"

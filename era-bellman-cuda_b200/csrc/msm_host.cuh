@@ -1,0 +1,40 @@
+// Host-side entry points of the MSM pipeline (internal C++ interface below
+// the C ABI).
+#pragma once
+
+#include "bellman-cuda-b200.h"
+#include "msm_kernels.cuh"
+#include <cuda_runtime.h>
+
+namespace msm_b200 {
+
+// One MSM request: device or host buffers, any count >= 1.
+struct execution {
+  cudaMemPool_t pool;
+  cudaStream_t stream;
+  const void *bases;
+  const void *scalars;
+  void *results; // 254 Jacobian points
+  unsigned count;
+  unsigned window_bits; // 0 = default for the size
+  cudaEvent_t h2d_event;
+  cudaHostFn_t h2d_callback;
+  void *h2d_callback_data;
+  cudaEvent_t d2h_event;
+  cudaHostFn_t d2h_callback;
+  void *d2h_callback_data;
+  msm_b200_profile *profile;       // optional: synchronous run with stage times and work counts
+  const cudaEvent_t *stage_events; // optional: PROFILE_STAGES + 1 caller events recorded at stage boundaries
+  unsigned *launches;              // optional: kernels enqueued
+};
+
+// stages timed by msm_b200_execute_profiled
+constexpr unsigned PROFILE_STAGES = 6;
+
+unsigned default_window_bits(unsigned long long n);
+plan make_plan(unsigned n, unsigned window_bits, int sms);
+size_t scratch_bytes(unsigned n, unsigned window_bits, bool copy_scalars, bool copy_bases, bool copy_results);
+cudaError_t execute(const execution &e);
+cudaError_t set_up();
+
+} // namespace msm_b200

@@ -1,0 +1,529 @@
+// Device kernels of the Pippenger MSM pipeline; see msm_kernels.cuh for the
+// overall data flow.
+#include "msm_kernels.cuh"
+
+namespace msm_b200 {
+
+// ---------------------------------------------------------------------------
+// 128-bit vector memory helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ fe load_fe_streaming(const fe *p) {
+  const uint4 *q = reinterpret_cast<const uint4 *>(p);
+  const uint4 a = __ldcs(q), b = __ldcs(q + 1);
+  fe r;
+  r.l[0] = a.x, r.l[1] = a.y, r.l[2] = a.z, r.l[3] = a.w;
+  r.l[4] = b.x, r.l[5] = b.y, r.l[6] = b.z, r.l[7] = b.w;
+  return r;
+}
+
+__device__ __forceinline__ affine load_affine(const affine *p) {
+  const uint4 *q = reinterpret_cast<const uint4 *>(p);
+  const uint4 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2), d = __ldg(q + 3);
+  affine r;
+  r.x.l[0] = a.x, r.x.l[1] = a.y, r.x.l[2] = a.z, r.x.l[3] = a.w;
+  r.x.l[4] = b.x, r.x.l[5] = b.y, r.x.l[6] = b.z, r.x.l[7] = b.w;
+  r.y.l[0] = c.x, r.y.l[1] = c.y, r.y.l[2] = c.z, r.y.l[3] = c.w;
+  r.y.l[4] = d.x, r.y.l[5] = d.y, r.y.l[6] = d.z, r.y.l[7] = d.w;
+  return r;
+}
+
+__device__ __forceinline__ xyzz load_xyzz(const xyzz *p) {
+  const uint4 *q = reinterpret_cast<const uint4 *>(p);
+  xyzz r;
+  uint32_t *w = reinterpret_cast<uint32_t *>(&r);
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    const uint4 v = q[i];
+    w[4 * i + 0] = v.x;
+    w[4 * i + 1] = v.y;
+    w[4 * i + 2] = v.z;
+    w[4 * i + 3] = v.w;
+  }
+  return r;
+}
+
+__device__ __forceinline__ void store_xyzz(xyzz *p, const xyzz &v) {
+  uint4 *q = reinterpret_cast<uint4 *>(p);
+  const uint32_t *w = reinterpret_cast<const uint32_t *>(&v);
+#pragma unroll
+  for (int i = 0; i < 8; i++)
+    q[i] = make_uint4(w[4 * i], w[4 * i + 1], w[4 * i + 2], w[4 * i + 3]);
+}
+
+__device__ __forceinline__ void store_jacobian(jacobian *p, const jacobian &v) {
+  uint4 *q = reinterpret_cast<uint4 *>(p);
+  const uint32_t *w = reinterpret_cast<const uint32_t *>(&v);
+#pragma unroll
+  for (int i = 0; i < 6; i++)
+    q[i] = make_uint4(w[4 * i], w[4 * i + 1], w[4 * i + 2], w[4 * i + 3]);
+}
+
+__device__ __forceinline__ uint32_t limb_at(const fe &s, unsigned k) {
+  uint32_t r = 0;
+#pragma unroll
+  for (unsigned j = 0; j < 8; j++)
+    r = (k == j) ? s.l[j] : r;
+  return r;
+}
+
+// ---------------------------------------------------------------------------
+// 1. digits
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) digits_kernel(const fe *__restrict__ scalars, unsigned n, unsigned c, unsigned windows,
+                                                     uint32_t *__restrict__ keys, uint32_t *__restrict__ vals) {
+  const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n)
+    return;
+  fe s = fr::from_mont(load_fe_streaming(scalars + i)); // canonical, < r
+  // r - s (s == 0 gives r, which is never the smaller one)
+  const fe m = fr::modulus();
+  fe neg;
+  neg.l[0] = bn254::cc::sub_cc(m.l[0], s.l[0]);
+#pragma unroll
+  for (int k = 1; k < 8; k++)
+    neg.l[k] = bn254::cc::subc_cc(m.l[k], s.l[k]);
+  const bool flip = fr::lt(neg, s);
+  if (flip)
+    s = neg;
+  const uint32_t half = 1u << (c - 1);
+  const uint32_t mask = (1u << c) - 1;
+  uint32_t carry = 0;
+  for (unsigned w = 0; w < windows; w++) {
+    const unsigned bit = w * c;
+    const unsigned limb = bit >> 5;
+    const uint32_t lo = limb < 8 ? limb_at(s, limb) : 0;
+    const uint32_t hi = limb + 1 < 8 ? limb_at(s, limb + 1) : 0;
+    uint32_t raw = (__funnelshift_r(lo, hi, bit & 31) & mask) + carry;
+    uint32_t negative = 0;
+    if (raw > half) {
+      raw = (mask + 1) - raw;
+      negative = 1;
+      carry = 1;
+    } else {
+      carry = 0;
+    }
+    const size_t out = (size_t)w * n + i;
+    keys[out] = raw;
+    vals[out] = i | ((negative ^ (flip ? 1u : 0u)) << 31);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 2. LSD radix sort, one 8-bit digit per pass, independent per window segment.
+//    counts / offsets layout per window: [digit][tile], so one exclusive scan
+//    of a window's array yields every (digit, tile) output offset.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(SORT_THREADS) sort_histogram_kernel(const uint32_t *__restrict__ keys, unsigned n, unsigned tiles,
+                                                                      unsigned shift, uint32_t *__restrict__ counts) {
+  __shared__ uint32_t hist[SORT_RADIX];
+  const unsigned tile = blockIdx.x, w = blockIdx.y;
+  for (unsigned d = threadIdx.x; d < SORT_RADIX; d += blockDim.x)
+    hist[d] = 0;
+  __syncthreads();
+  const uint32_t *seg = keys + (size_t)w * n;
+  const unsigned lane = threadIdx.x & 31;
+#pragma unroll 4
+  for (unsigned k = 0; k < SORT_ITEMS; k++) {
+    const unsigned idx = tile * SORT_TILE + k * SORT_THREADS + threadIdx.x;
+    const unsigned d = idx < n ? (seg[idx] >> shift) & (SORT_RADIX - 1) : SORT_RADIX;
+    // warp-aggregated increment: one shared atomic per distinct digit
+    const unsigned peers = __match_any_sync(0xffffffffu, d);
+    if (d < SORT_RADIX && lane == (unsigned)(__ffs(peers) - 1))
+      atomicAdd(&hist[d], (unsigned)__popc(peers));
+  }
+  __syncthreads();
+  for (unsigned d = threadIdx.x; d < SORT_RADIX; d += blockDim.x)
+    counts[((size_t)w * SORT_RADIX + d) * tiles + tile] = hist[d];
+}
+
+// Exclusive scan of one window's [digit][tile] counts; one block per window.
+__global__ void __launch_bounds__(1024) sort_scan_kernel(uint32_t *counts, unsigned tiles) {
+  __shared__ uint32_t warp_sums[32];
+  __shared__ uint32_t carry_in;
+  const unsigned total = SORT_RADIX * tiles;
+  uint32_t *seg = counts + (size_t)blockIdx.x * total;
+  if (threadIdx.x == 0)
+    carry_in = 0;
+  __syncthreads();
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (unsigned base = 0; base < total; base += 4 * blockDim.x) {
+    uint32_t v[4];
+    uint32_t local = 0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const unsigned idx = base + 4 * threadIdx.x + k;
+      v[k] = idx < total ? seg[idx] : 0;
+      local += v[k];
+    }
+    // inclusive warp scan of the per-thread sums
+    uint32_t incl = local;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, incl, off);
+      if (lane >= (unsigned)off)
+        incl += t;
+    }
+    if (lane == 31)
+      warp_sums[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+      uint32_t ws = lane < (blockDim.x >> 5) ? warp_sums[lane] : 0;
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, ws, off);
+        if (lane >= (unsigned)off)
+          ws += t;
+      }
+      warp_sums[lane] = ws; // inclusive
+    }
+    __syncthreads();
+    uint32_t run = carry_in + (incl - local) + (warp > 0 ? warp_sums[warp - 1] : 0);
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const unsigned idx = base + 4 * threadIdx.x + k;
+      if (idx < total)
+        seg[idx] = run;
+      run += v[k];
+    }
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1)
+      carry_in = run;
+    __syncthreads();
+  }
+}
+
+// Stable scatter.  Warp k of the block ranks the items of its sub-tile round by
+// round (32 consecutive items per round) with __match_any_sync; per-warp digit
+// counters then get an exclusive scan across warps and the tile's global
+// offset, which keeps the pass stable.
+__global__ void __launch_bounds__(SORT_THREADS) sort_scatter_kernel(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
+                                                                    uint32_t *__restrict__ keys_out, uint32_t *__restrict__ vals_out,
+                                                                    unsigned n, unsigned tiles, unsigned shift,
+                                                                    const uint32_t *__restrict__ offsets) {
+  constexpr unsigned WARPS = SORT_THREADS / 32;
+  __shared__ uint32_t whist[WARPS][SORT_RADIX];
+  const unsigned tile = blockIdx.x, w = blockIdx.y;
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (unsigned d = lane; d < SORT_RADIX; d += 32)
+    whist[warp][d] = 0;
+  __syncwarp();
+  const size_t seg = (size_t)w * n;
+  const unsigned sub_base = tile * SORT_TILE + warp * (32 * SORT_ITEMS);
+  const unsigned lt_mask = (1u << lane) - 1;
+  uint32_t key[SORT_ITEMS], val[SORT_ITEMS], rank[SORT_ITEMS];
+#pragma unroll
+  for (unsigned r = 0; r < SORT_ITEMS; r++) {
+    const unsigned idx = sub_base + r * 32 + lane;
+    const bool valid = idx < n;
+    key[r] = valid ? keys_in[seg + idx] : 0;
+    val[r] = valid ? vals_in[seg + idx] : 0;
+    const unsigned d = valid ? (key[r] >> shift) & (SORT_RADIX - 1) : SORT_RADIX;
+    const unsigned peers = __match_any_sync(0xffffffffu, d);
+    const uint32_t before = valid ? whist[warp][d] : 0;
+    __syncwarp();
+    if (valid && lane == (unsigned)(__ffs(peers) - 1))
+      whist[warp][d] = before + __popc(peers);
+    __syncwarp();
+    rank[r] = before + __popc(peers & lt_mask);
+  }
+  __syncthreads();
+  for (unsigned d = threadIdx.x; d < SORT_RADIX; d += blockDim.x) {
+    uint32_t run = offsets[((size_t)w * SORT_RADIX + d) * tiles + tile];
+#pragma unroll
+    for (unsigned k = 0; k < WARPS; k++) {
+      const uint32_t t = whist[k][d];
+      whist[k][d] = run;
+      run += t;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (unsigned r = 0; r < SORT_ITEMS; r++) {
+    const unsigned idx = sub_base + r * 32 + lane;
+    if (idx < n) {
+      const unsigned d = (key[r] >> shift) & (SORT_RADIX - 1);
+      const uint32_t pos = whist[warp][d] + rank[r];
+      keys_out[seg + pos] = key[r];
+      vals_out[seg + pos] = val[r];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 3. first nonzero key of each sorted window
+// ---------------------------------------------------------------------------
+__global__ void zero_counts_kernel(const uint32_t *__restrict__ keys, unsigned n, unsigned windows, uint32_t *__restrict__ zeros) {
+  const unsigned w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= windows)
+    return;
+  const uint32_t *seg = keys + (size_t)w * n;
+  unsigned lo = 0, hi = n; // first index with key != 0
+  while (lo < hi) {
+    const unsigned mid = (lo + hi) >> 1;
+    if (seg[mid] == 0)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  zeros[w] = lo;
+}
+
+// ---------------------------------------------------------------------------
+// 4. accumulation
+// ---------------------------------------------------------------------------
+constexpr unsigned MAX_WINDOWS = 128;
+
+struct entry_cursor {
+  size_t idx;       // physical index into keys / vals
+  unsigned w;       // window of idx
+  size_t seg_end;   // (w + 1) * n
+};
+
+__device__ __forceinline__ void cursor_advance(entry_cursor &cur, unsigned n, unsigned windows, const uint32_t *s_zeros) {
+  cur.idx++;
+  if (cur.idx == cur.seg_end) {
+    unsigned w = cur.w + 1;
+    while (w < windows && s_zeros[w] == n)
+      w++;
+    cur.w = w;
+    cur.seg_end = (size_t)(w + 1) * n;
+    cur.idx = (size_t)w * n + (w < windows ? s_zeros[w] : 0);
+  }
+}
+
+__device__ __forceinline__ affine signed_base(const affine *__restrict__ bases, uint32_t val) {
+  affine p = load_affine(bases + (val & 0x7fffffffu));
+  if (val >> 31)
+    p.y = fq::neg(p.y);
+  return p;
+}
+
+__global__ void __launch_bounds__(ACC_THREADS) accumulate_kernel(const uint32_t *__restrict__ keys, const uint32_t *__restrict__ vals,
+                                                                 const affine *__restrict__ bases, unsigned n, unsigned windows, unsigned log_b,
+                                                                 const uint32_t *__restrict__ zeros, unsigned total_threads,
+                                                                 xyzz *__restrict__ buckets, uint8_t *__restrict__ flags,
+                                                                 uint32_t *__restrict__ head_bucket, xyzz *__restrict__ head_point) {
+  __shared__ uint32_t s_zeros[MAX_WINDOWS];
+  __shared__ unsigned long long s_prefix[MAX_WINDOWS + 1];
+  for (unsigned w = threadIdx.x; w < windows; w += blockDim.x)
+    s_zeros[w] = zeros[w];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long acc = 0;
+    for (unsigned w = 0; w < windows; w++) {
+      s_prefix[w] = acc;
+      acc += n - s_zeros[w];
+    }
+    s_prefix[windows] = acc;
+  }
+  __syncthreads();
+  const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= total_threads)
+    return;
+  const unsigned long long total = s_prefix[windows];
+  const unsigned long long beg = total * t / total_threads;
+  const unsigned long long end = total * (t + 1) / total_threads;
+  head_bucket[t] = INVALID_BUCKET;
+  if (beg == end)
+    return;
+  unsigned w = 0;
+  while (w + 1 < windows && s_prefix[w + 1] <= beg)
+    w++;
+  entry_cursor cur;
+  cur.w = w;
+  cur.seg_end = (size_t)(w + 1) * n;
+  cur.idx = (size_t)w * n + s_zeros[w] + (size_t)(beg - s_prefix[w]);
+  const uint32_t slot_mask = (1u << log_b) - 1;
+
+  uint32_t key = keys[cur.idx];
+  uint32_t val = vals[cur.idx];
+  // does this range start in the middle of a bucket?
+  const bool continued = cur.idx > (size_t)w * n + s_zeros[w] && keys[cur.idx - 1] == key;
+  unsigned bucket = (cur.w << log_b) | (key & slot_mask);
+  xyzz acc = curve::from_affine(signed_base(bases, val));
+  bool first = true;
+  const unsigned long long count = end - beg;
+  for (unsigned long long k = 1; k < count; k++) {
+    cursor_advance(cur, n, windows, s_zeros);
+    key = keys[cur.idx];
+    val = vals[cur.idx];
+    const unsigned b = (cur.w << log_b) | (key & slot_mask);
+    const affine p = signed_base(bases, val);
+    if (b != bucket) {
+      if (first && continued) {
+        head_bucket[t] = bucket;
+        store_xyzz(head_point + t, acc);
+      } else {
+        store_xyzz(buckets + bucket, acc);
+        flags[bucket] = 1;
+      }
+      first = false;
+      bucket = b;
+      acc = curve::from_affine(p);
+    } else {
+      acc = curve::add_affine(acc, p);
+    }
+  }
+  if (first && continued) {
+    head_bucket[t] = bucket;
+    store_xyzz(head_point + t, acc);
+  } else {
+    store_xyzz(buckets + bucket, acc);
+    flags[bucket] = 1;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 5. fold head partial sums into their buckets
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(ACC_THREADS) merge_heads_kernel(const uint32_t *__restrict__ hb_in, const xyzz *__restrict__ hp_in,
+                                                                  unsigned n_in, unsigned chunk, xyzz *__restrict__ buckets,
+                                                                  uint32_t *__restrict__ hb_out, xyzz *__restrict__ hp_out) {
+  const unsigned u = blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned long long beg = (unsigned long long)u * chunk;
+  if (beg >= n_in)
+    return;
+  const unsigned end = (unsigned)min((unsigned long long)n_in, beg + chunk);
+  hb_out[u] = INVALID_BUCKET;
+  unsigned bucket = INVALID_BUCKET;
+  bool head_is_continuation = false, seen = false;
+  xyzz acc;
+  for (unsigned k = (unsigned)beg; k < end; k++) {
+    const unsigned b = hb_in[k];
+    if (b == INVALID_BUCKET)
+      continue;
+    const xyzz p = load_xyzz(hp_in + k);
+    if (b != bucket) {
+      if (bucket != INVALID_BUCKET) {
+        if (head_is_continuation) {
+          hb_out[u] = bucket;
+          store_xyzz(hp_out + u, acc);
+        } else {
+          store_xyzz(buckets + bucket, curve::add(load_xyzz(buckets + bucket), acc));
+        }
+      }
+      head_is_continuation = !seen && k == beg && k > 0 && hb_in[k - 1] == b;
+      seen = true;
+      bucket = b;
+      acc = p;
+    } else {
+      acc = curve::add(acc, p);
+    }
+  }
+  if (bucket != INVALID_BUCKET) {
+    if (head_is_continuation) {
+      hb_out[u] = bucket;
+      store_xyzz(hp_out + u, acc);
+    } else {
+      store_xyzz(buckets + bucket, curve::add(load_xyzz(buckets + bucket), acc));
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 6. reduction
+// ---------------------------------------------------------------------------
+// Stream layout per window (stride 2G): stream 0 = the G group sums "acc",
+// stream s >= 1 = the G >> s odd entries of tree level s - 1.
+__host__ __device__ __forceinline__ unsigned stream_offset(unsigned log_g, unsigned s) {
+  const unsigned g = 1u << log_g;
+  return s == 0 ? 0 : g + (g - (g >> (s - 1)));
+}
+
+__host__ __device__ __forceinline__ unsigned stream_length(unsigned log_g, unsigned s) { return s == 0 ? (1u << log_g) : (1u << log_g) >> s; }
+
+// Thread (w, g): slots k = g*m + i of window w, weights k (slot 0 of a window
+// holds |d| = B and is excluded here).  For i = m-1 .. 1: run += X, acc += run,
+// giving acc = sum_i i * X_{gm+i} and run = sum_i X_{gm+i}; then
+// S_w = sum_g acc_g + m * sum_g g * run_g.
+__global__ void __launch_bounds__(ACC_THREADS) reduce_groups_kernel(const xyzz *__restrict__ buckets, const uint8_t *__restrict__ flags,
+                                                                    unsigned windows, unsigned log_b, unsigned log_m, xyzz *__restrict__ run_out,
+                                                                    xyzz *__restrict__ streams) {
+  const unsigned log_g = log_b - log_m;
+  const unsigned gid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= (windows << log_g))
+    return;
+  const unsigned w = gid >> log_g, g = gid & ((1u << log_g) - 1);
+  const unsigned base = (w << log_b) + (g << log_m);
+  xyzz run = curve::infinity(), acc = curve::infinity();
+  for (unsigned i = (1u << log_m) - 1; i >= 1; i--) {
+    if (flags[base + i])
+      run = curve::add(run, load_xyzz(buckets + base + i));
+    acc = curve::add(acc, run);
+  }
+  if (g > 0 && flags[base])
+    run = curve::add(run, load_xyzz(buckets + base));
+  store_xyzz(run_out + gid, run);
+  store_xyzz(streams + (size_t)w * stream_stride(log_g) + stream_offset(log_g, 0) + g, acc);
+}
+
+// Tree level `level`: T_{level} has G >> level entries per window (stride G).
+// Odd entries go to stream level + 1; pair sums form T_{level+1}.
+__global__ void __launch_bounds__(ACC_THREADS) reduce_tree_kernel(const xyzz *__restrict__ t_in, xyzz *__restrict__ t_out,
+                                                                  xyzz *__restrict__ streams, unsigned windows, unsigned log_g,
+                                                                  unsigned level) {
+  const unsigned half = (1u << log_g) >> (level + 1);
+  const unsigned gid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= windows * half)
+    return;
+  const unsigned w = gid / half, i = gid % half;
+  const size_t g = (size_t)1 << log_g;
+  const xyzz a = load_xyzz(t_in + w * g + 2 * i);
+  const xyzz b = load_xyzz(t_in + w * g + 2 * i + 1);
+  store_xyzz(streams + (size_t)w * stream_stride(log_g) + stream_offset(log_g, level + 1) + i, b);
+  if (level + 1 < log_g)
+    store_xyzz(t_out + w * g + i, curve::add(a, b));
+}
+
+// One plain-sum pass: every stream of length L (as of divisor_in) shrinks to
+// ceil(L / fanin); layout unchanged.
+__global__ void __launch_bounds__(ACC_THREADS) reduce_streams_kernel(const xyzz *__restrict__ in, xyzz *__restrict__ out, unsigned windows,
+                                                                     unsigned log_g, unsigned fanin, unsigned divisor_in) {
+  const unsigned streams_per_window = log_g + 1;
+  const unsigned sid = blockIdx.y;
+  const unsigned w = sid / streams_per_window, s = sid % streams_per_window;
+  if (w >= windows)
+    return;
+  const unsigned len0 = stream_length(log_g, s);
+  const unsigned len_in = (len0 + divisor_in - 1) / divisor_in;
+  const unsigned len_out = (len_in + fanin - 1) / fanin;
+  const unsigned q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= len_out)
+    return;
+  const size_t base = (size_t)w * stream_stride(log_g) + stream_offset(log_g, s);
+  xyzz acc = curve::infinity();
+  for (unsigned f = 0; f < fanin; f++) {
+    const unsigned k = q * fanin + f;
+    if (k < len_in)
+      acc = curve::add(acc, load_xyzz(in + base + k));
+  }
+  store_xyzz(out + base + q, acc);
+}
+
+// Result bit i = c*w + o:  o == 0 -> stream 0;  o == c-1 -> slot 0 (|d| = B);
+// log_m <= o < c-1 -> stream o - log_m + 1;  otherwise infinity.
+__global__ void gather_results_kernel(const xyzz *__restrict__ streams, const xyzz *__restrict__ buckets, const uint8_t *__restrict__ flags,
+                                      unsigned windows, unsigned c, unsigned log_m, unsigned log_g, unsigned divisor,
+                                      jacobian *__restrict__ results) {
+  (void)divisor;
+  const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= RESULT_BITS)
+    return;
+  const unsigned w = i / c, o = i % c;
+  xyzz p = curve::infinity();
+  if (w < windows) {
+    const size_t base = (size_t)w * stream_stride(log_g);
+    if (o == 0) {
+      p = load_xyzz(streams + base + stream_offset(log_g, 0));
+    } else if (o == c - 1) {
+      const unsigned slot0 = w << (c - 1);
+      if (flags[slot0])
+        p = load_xyzz(buckets + slot0);
+    } else if (o >= log_m && o - log_m < log_g) {
+      p = load_xyzz(streams + base + stream_offset(log_g, o - log_m + 1));
+    }
+  }
+  store_jacobian(results + i, curve::to_jacobian(p));
+}
+
+} // namespace msm_b200

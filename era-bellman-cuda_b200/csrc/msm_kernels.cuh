@@ -1,0 +1,119 @@
+// Device kernels of the Pippenger MSM pipeline (one GPU, sm_100a).
+//
+// Pipeline for n points, window width c, W = ceil(254 / c) windows and
+// B = 2^(c-1) bucket slots per window:
+//   1. digits      scalars -> signed c-bit digits of min(s, r - s); per window
+//                  a key |d| in [0, B] and a value (point index | sign << 31)
+//   2. sort        LSD radix sort of (key, value) inside each window segment
+//   3. zero_counts first nonzero key of every window (zero digits sort first)
+//   4. accumulate  the nonzero entries of all windows are split into equal
+//                  contiguous ranges, one per thread; each thread adds its
+//                  range bucket by bucket (XYZZ += affine); buckets that start
+//                  inside a range are written directly, a bucket continued
+//                  from the previous range leaves a "head" partial sum
+//   5. merge_heads heads of one bucket are contiguous; chunked, repeated
+//                  until every head is folded into its bucket
+//   6. reduction   per window S_w = sum_k k * X_k (X_k = bucket of |d| = k,
+//                  slot 0 holds |d| = B): running sums over groups of m slots,
+//                  then a binary decomposition of the group weights, so every
+//                  partial result is a plain sum placed at the bit position it
+//                  belongs to in the 254-entry result array.
+// The caller's Horner pass over the 254 results (sum 2^i R_i) completes the
+// MSM, exactly as with the reference (src/bellman-cuda.h:496-505).
+#pragma once
+
+#include "bn254_curve.cuh"
+#include <cuda_runtime.h>
+
+namespace msm_b200 {
+
+using bn254::affine;
+using bn254::curve;
+using bn254::fe;
+using bn254::fq;
+using bn254::fr;
+using bn254::jacobian;
+using bn254::xyzz;
+
+constexpr unsigned RESULT_BITS = 254;
+constexpr unsigned INVALID_BUCKET = 0xffffffffu;
+constexpr unsigned SORT_RADIX_BITS = 8;
+constexpr unsigned SORT_RADIX = 1u << SORT_RADIX_BITS;
+constexpr unsigned SORT_THREADS = 256;
+constexpr unsigned SORT_ITEMS = 16; // per thread; a tile is SORT_THREADS * SORT_ITEMS keys
+constexpr unsigned SORT_TILE = SORT_THREADS * SORT_ITEMS;
+constexpr unsigned ACC_THREADS = 128;
+
+// Launch geometry of the whole pipeline, computed on the host.
+struct plan {
+  unsigned n;           // points
+  unsigned c;           // window bits
+  unsigned windows;     // W
+  unsigned log_b;       // log2 of bucket slots per window (c - 1)
+  unsigned key_bits;    // bits of a key (keys are in [0, 2^log_b])
+  unsigned sort_passes; // radix passes
+  unsigned tiles;       // sort tiles per window
+  unsigned acc_threads; // accumulation threads (ranges)
+  unsigned merge_chunk; // heads per merge thread
+  unsigned log_m;       // log2 of the running-sum group
+  unsigned groups;      // G = B / m groups per window
+  unsigned log_g;       // gamma = log2 G
+  unsigned sum_fanin;   // fan-in of the plain-sum passes
+};
+
+// ---------------------------------------------------------------------------
+// 1. digits
+// ---------------------------------------------------------------------------
+// Signed windows of s' = min(s, r - s) < 2^253 (reference fold,
+// src/msm_kernels.cu:49-52): raw = bits [c*w, c*w + c) + carry; a raw value
+// above B becomes raw - 2^c with a carry into the next window.  |d| <= B,
+// and the top window of a W*c >= 254 split never carries out.
+__global__ void digits_kernel(const fe *__restrict__ scalars, unsigned n, unsigned c, unsigned windows, uint32_t *__restrict__ keys,
+                              uint32_t *__restrict__ vals);
+
+// ---------------------------------------------------------------------------
+// 2. sort (keys and values per window segment of n entries)
+// ---------------------------------------------------------------------------
+__global__ void sort_histogram_kernel(const uint32_t *__restrict__ keys, unsigned n, unsigned tiles, unsigned shift,
+                                      uint32_t *__restrict__ counts);
+__global__ void sort_scan_kernel(uint32_t *counts, unsigned tiles);
+__global__ void sort_scatter_kernel(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in, uint32_t *__restrict__ keys_out,
+                                    uint32_t *__restrict__ vals_out, unsigned n, unsigned tiles, unsigned shift,
+                                    const uint32_t *__restrict__ offsets);
+
+// ---------------------------------------------------------------------------
+// 3. zero counts
+// ---------------------------------------------------------------------------
+__global__ void zero_counts_kernel(const uint32_t *__restrict__ keys, unsigned n, unsigned windows, uint32_t *__restrict__ zeros);
+
+// ---------------------------------------------------------------------------
+// 4. accumulation
+// ---------------------------------------------------------------------------
+__global__ void accumulate_kernel(const uint32_t *__restrict__ keys, const uint32_t *__restrict__ vals, const affine *__restrict__ bases,
+                                  unsigned n, unsigned windows, unsigned log_b, const uint32_t *__restrict__ zeros, unsigned total_threads,
+                                  xyzz *__restrict__ buckets, uint8_t *__restrict__ flags, uint32_t *__restrict__ head_bucket,
+                                  xyzz *__restrict__ head_point);
+
+// ---------------------------------------------------------------------------
+// 5. heads
+// ---------------------------------------------------------------------------
+__global__ void merge_heads_kernel(const uint32_t *__restrict__ hb_in, const xyzz *__restrict__ hp_in, unsigned n_in, unsigned chunk,
+                                   xyzz *__restrict__ buckets, uint32_t *__restrict__ hb_out, xyzz *__restrict__ hp_out);
+
+// ---------------------------------------------------------------------------
+// 6. reduction
+// ---------------------------------------------------------------------------
+__global__ void reduce_groups_kernel(const xyzz *__restrict__ buckets, const uint8_t *__restrict__ flags, unsigned windows, unsigned log_b,
+                                     unsigned log_m, xyzz *__restrict__ run, xyzz *__restrict__ streams);
+__global__ void reduce_tree_kernel(const xyzz *__restrict__ t_in, xyzz *__restrict__ t_out, xyzz *__restrict__ streams, unsigned windows,
+                                   unsigned log_g, unsigned level);
+__global__ void reduce_streams_kernel(const xyzz *__restrict__ in, xyzz *__restrict__ out, unsigned windows, unsigned log_g, unsigned fanin,
+                                      unsigned divisor_in);
+__global__ void gather_results_kernel(const xyzz *__restrict__ streams, const xyzz *__restrict__ buckets, const uint8_t *__restrict__ flags,
+                                      unsigned windows, unsigned c, unsigned log_m, unsigned log_g, unsigned divisor,
+                                      jacobian *__restrict__ results);
+
+// stride of the per-window plain-sum streams (stream 0: G entries, stream s: G >> s)
+__host__ __device__ __forceinline__ size_t stream_stride(unsigned log_g) { return (size_t)2 << log_g; }
+
+} // namespace msm_b200

@@ -1,0 +1,78 @@
+/*
+ * bellman-cuda-b200.h -- extensions of the B200 MSM library beyond the
+ * era-bellman-cuda ABI (which is declared, unchanged, in bellman-cuda.h).
+ * None of these has a counterpart in the reference.
+ */
+#pragma once
+
+#include "bellman-cuda.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#pragma GCC visibility push(default) /* the library builds with hidden visibility */
+#endif
+
+/* An MSM of any length (the reference's msm_execute_async takes powers of two
+ * only).  Same buffers and result convention as msm_execute_async. */
+typedef struct msm_b200_configuration {
+  bc_mem_pool mem_pool; /* may be a null handle: the device's default pool */
+  bc_stream stream;
+  const void *bases;    /* count affine points, Montgomery form, 64 B each */
+  const void *scalars;  /* count Montgomery-form scalars, 32 B each */
+  void *results;        /* 254 Jacobian points, MSM = sum_i 2^i R_i */
+  unsigned count;       /* >= 1 */
+  unsigned window_bits; /* 0: size-based default; otherwise 2..24 */
+} msm_b200_configuration;
+
+bc_error msm_b200_execute_async(const msm_b200_configuration *configuration);
+
+/* Per-stage device times and work counts of one MSM. */
+typedef struct msm_b200_profile {
+  float stage_ms[6];                   /* digits, sort, zero counts, accumulation, head merge, bucket reduction */
+  unsigned long long nonzero_entries;  /* (window, point) pairs with a nonzero digit */
+  unsigned long long nonempty_buckets; /* buckets that received at least one point */
+  unsigned long long heads;            /* accumulation ranges that began inside a bucket */
+  unsigned window_bits, windows, acc_threads, launches;
+} msm_b200_profile;
+
+/* Same as msm_b200_execute_async, but synchronises the stream before it
+ * returns and fills *profile.  Mixed additions performed by the accumulation
+ * kernel = nonzero_entries - nonempty_buckets - heads. */
+bc_error msm_b200_execute_profiled(const msm_b200_configuration *configuration, msm_b200_profile *profile);
+
+/* msm_b200_execute_async that also records stage_events[0..6] on the stream:
+ * before the first stage and after each of the six stages of
+ * msm_b200_profile.stage_ms (no synchronisation).  *launches (optional)
+ * receives the number of kernels enqueued. */
+bc_error msm_b200_execute_staged_async(const msm_b200_configuration *configuration, const bc_event *stage_events, unsigned *launches);
+
+/* Throughput of 32-bit multiply instructions on the current device, in
+ * multiply instructions per second (mul.lo / mul.hi / mad* each count one):
+ *   kind 0: independent mad.lo / mad.hi (the integer multiply pipe's peak)
+ *   kind 1: carry chains of madc.lo.cc / madc.hi.cc pairs
+ *   kind 2: Fq Montgomery products (264 multiply instructions each)
+ *   kind 3: XYZZ + affine mixed additions (2392 multiply instructions each)
+ * Synchronous; about 0.1 s. */
+bc_error msm_b200_measure_mul_throughput(unsigned kind, double *mulops_per_second);
+
+/* Bytes of pool memory one device-resident MSM of `count` points takes. */
+bc_error msm_b200_scratch_bytes(unsigned count, unsigned window_bits, size_t *bytes);
+
+/* The window width msm_execute_async uses for `count` points. */
+bc_error msm_b200_default_window_bits(unsigned count, unsigned *window_bits);
+
+/* bases[i] = k[i] * G for the generator G = (1, 2), as Montgomery-form affine
+ * points (64 B each).  k: `count` standard-form scalars in [1, r), device
+ * memory.  Used to build synthetic base tables on the device. */
+bc_error msm_b200_generator_multiples_async(const void *k, void *bases, unsigned count, bc_stream stream);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif

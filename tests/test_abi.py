@@ -1,0 +1,93 @@
+"""The C-ABI library: loads without a GPU, exports every function the headers
+in include/ declare, and its ctypes mirror matches the C struct layout (and the
+reference header's layout when the reference tree is present)."""
+import ctypes
+import os
+import re
+import subprocess
+
+import pytest
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+INCLUDE = os.path.join(REPO, "include")
+REF_HEADER = "/root/reference/src/bellman-cuda.h"
+
+
+def declared_functions():
+    names = set()
+    for h in ("bellman-cuda.h", "bellman-cuda-b200.h"):
+        text = open(os.path.join(INCLUDE, h)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names |= set(re.findall(r"^bc_error\s+(\w+)\s*\(", text, flags=re.M))
+    return sorted(names)
+
+
+def test_library_exports_every_declared_symbol(product_lib_path):
+    lib = ctypes.CDLL(product_lib_path)
+    names = declared_functions()
+    assert len(names) >= 40
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_reference_msm_surface_is_declared():
+    """Every MSM-path function of the reference ABI appears in include/bellman-cuda.h."""
+    names = set(declared_functions())
+    required = """bc_get_device_count bc_get_device bc_set_device bc_stream_create bc_stream_wait_event
+    bc_stream_synchronize bc_stream_query bc_stream_destroy bc_launch_host_fn bc_event_create bc_event_record
+    bc_event_synchronize bc_event_query bc_event_destroy bc_event_elapsed_time bc_mem_get_info bc_malloc
+    bc_malloc_host bc_free bc_free_host bc_host_register bc_host_unregister bc_device_disable_peer_access
+    bc_device_enable_peer_access bc_memcpy bc_memcpy_async bc_memset bc_memset_async bc_mem_pool_create
+    bc_mem_pool_destroy bc_mem_pool_disable_peer_access bc_mem_pool_enable_peer_access bc_malloc_from_pool_async
+    bc_free_async ff_set_up msm_set_up msm_execute_async msm_tear_down""".split()
+    assert not [n for n in required if n not in names]
+
+
+LAYOUT_PROGRAM = r"""
+#include <stdio.h>
+#include <stddef.h>
+#include "bellman-cuda.h"
+int main(void) {
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu %d %d %d %d\n", sizeof(msm_configuration),
+         offsetof(msm_configuration, bases), offsetof(msm_configuration, scalars),
+         offsetof(msm_configuration, results), offsetof(msm_configuration, log_scalars_count),
+         offsetof(msm_configuration, h2d_copy_finished), offsetof(msm_configuration, d2h_copy_finished),
+         offsetof(msm_configuration, d2h_copy_finished_callback_data),
+         (int)bc_success, (int)bc_error_invalid_value, (int)bc_error_memory_allocation, (int)bc_error_not_ready);
+  return 0;
+}
+"""
+
+
+def c_layout(include_dir, tmp_path, tag):
+    src = tmp_path / f"layout_{tag}.c"
+    exe = tmp_path / f"layout_{tag}"
+    src.write_text(LAYOUT_PROGRAM)
+    subprocess.run(["gcc", "-std=c11", "-I", include_dir, str(src), "-o", str(exe)], check=True)
+    return subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()
+
+
+def test_struct_layout_matches_ctypes(tmp_path):
+    import bellman_cuda as bc
+    got = c_layout(INCLUDE, tmp_path, "b200")
+    M = bc.MsmConfiguration
+    mine = [ctypes.sizeof(M), M.bases.offset, M.scalars.offset, M.results.offset, M.log_scalars_count.offset,
+            M.h2d_copy_finished.offset, M.d2h_copy_finished.offset, M.d2h_copy_finished_callback_data.offset, 0, 1, 2, 600]
+    assert [int(v) for v in got] == mine
+
+
+@pytest.mark.skipif(not os.path.exists(REF_HEADER), reason="reference tree absent")
+def test_struct_layout_matches_reference_header(tmp_path):
+    ref = c_layout(os.path.dirname(REF_HEADER), tmp_path, "ref")
+    mine = c_layout(INCLUDE, tmp_path, "b200")
+    assert ref == mine
+
+
+def test_reference_build_exports_same_msm_surface():
+    path = os.path.join(REPO, "oracle", "_ref", "libbellman-cuda-ref.so")
+    if not os.path.exists(path):
+        pytest.skip("reference GPU build absent")
+    out = subprocess.run(["nm", "-D", "--defined-only", path], check=True, capture_output=True, text=True).stdout
+    ref_syms = set(line.split()[-1] for line in out.splitlines())
+    mine = set(declared_functions())
+    assert {n for n in mine if not n.startswith("msm_b200_") and n != "ff_tear_down"} <= ref_syms

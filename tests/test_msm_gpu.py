@@ -1,0 +1,266 @@
+"""GPU parity of msm_execute_async (and the any-length extension) against the
+oracle, the golden fixtures and, when built, the reference's own sm_100a
+library on identical inputs.  Every comparison is bit-exact on the normalised
+affine point (standard form, fully reduced, infinity flagged), after the
+caller-side Horner reduction of the 254 results."""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+import msm_helpers as H
+import synth
+
+pytestmark = pytest.mark.gpu
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF_GPU = os.path.join(REPO, "oracle", "_ref", "libbellman-cuda-ref.so")
+
+
+class Runner:
+    """One library (ours or the reference) driven through the bellman-cuda ABI."""
+
+    def __init__(self, path=None):
+        import bellman_cuda as bcm
+        self.bc = bcm.BellmanCuda(path) if path else bcm.BellmanCuda()
+        self.bc.set_device(0)
+        self.bc.ff_set_up(25, 14)
+        self.bc.msm_set_up()
+        self.pool = self.bc.mem_pool_create(0)
+        self.stream = self.bc.stream_create(True)
+
+    def upload(self, a):
+        return self.bc.to_device(np.ascontiguousarray(a))
+
+    def msm(self, bases, scalars, log_n=None, scalars_mem="device", results_mem="device", bases_dev=None):
+        bc = self.bc
+        n = len(scalars)
+        if log_n is None:
+            log_n = max(0, (n - 1).bit_length())
+        full = 1 << log_n
+        if full != n:  # pad with zero scalars: zero digits contribute nothing
+            scalars = np.concatenate([scalars, np.zeros((full - n, 8), np.uint32)])
+            bases = np.concatenate([bases, np.repeat(bases[:1], full - n, axis=0)])
+        owned = []
+        if bases_dev is None:
+            bases_dev = self.upload(bases)
+            owned.append(bases_dev)
+        pinned = []
+        if scalars_mem == "device":
+            s = self.upload(scalars)
+            owned.append(s)
+        elif scalars_mem == "pinned":
+            s, ptr = bc.pinned_array(scalars.shape)
+            s[...] = scalars
+            pinned.append(ptr)
+        else:
+            s = np.ascontiguousarray(scalars)
+        results = np.zeros((254, 24), np.uint32)
+        if results_mem == "device":
+            r = bc.malloc(results.nbytes)
+            owned.append(r)
+        elif results_mem == "pinned":
+            r, ptr = bc.pinned_array((254, 24))
+            pinned.append(ptr)
+        else:
+            r = results
+        bc.msm(self.pool, self.stream, bases_dev, s, r, log_n)
+        bc.stream_synchronize(self.stream)
+        if results_mem == "device":
+            bc.memcpy(results, r, results.nbytes)
+        elif results_mem == "pinned":
+            results[...] = r
+        for p in owned:
+            bc.free(p)
+        for p in pinned:
+            bc.free_host(p)
+        return results
+
+
+@pytest.fixture(scope="module")
+def gpu():
+    return Runner()
+
+
+@pytest.fixture(scope="module")
+def ref_gpu():
+    if not os.path.exists(REF_GPU):
+        pytest.skip("reference sm_100a build absent (make -C oracle ref)")
+    return Runner(REF_GPU)
+
+
+def generated_bases(gpu, k):
+    """k_i * G on the device (extension kernel); returns (device pointer, host copy)."""
+    bc = gpu.bc
+    kd = gpu.upload(k)
+    bd = bc.malloc(len(k) * 64)
+    bc.generator_multiples(kd, bd, len(k), gpu.stream)
+    bc.stream_synchronize(gpu.stream)
+    bc.free(kd)
+    return bd, bc.from_device(bd, (len(k), 16))
+
+
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("case", H.load_json("msm_small.json")["cases"], ids=lambda c: c["name"])
+def test_small_golden(gpu, oracle, case):
+    table = H.load_g_bases()
+    bases = H.mont_point_array([table[i] for i in case["bases"]])
+    scalars = H.mont_scalar_array([int(s, 16) for s in case["scalars"]])
+    assert oracle.horner(gpu.msm(bases, scalars)) == H.expected_point(case)
+
+
+def test_config0_golden(gpu, oracle):
+    """N = 2^12, seed 0, bases k_i*G: the committed reference result."""
+    cfg = H.load_json("config0.json")
+    scalars, k = synth.workload("uniform", cfg["n"], cfg["seed"])
+    bases = oracle.gen_bases(k)
+    assert oracle.horner(gpu.msm(bases, scalars)) == H.expected_point(cfg)
+
+
+@pytest.mark.parametrize("log_n", [0, 1, 2, 3, 4, 5, 7, 8, 10, 11, 13, 14, 16])
+def test_sizes_table_bases(gpu, oracle, log_n):
+    """Reference-test style (tests/msm_test.cu:155-170): bases from the 256-point
+    table, so repeated bases exercise the doubling branches."""
+    bases, scalars, k = H.table_workload(1 << log_n, 10 + log_n)
+    assert oracle.horner(gpu.msm(bases, scalars)) == oracle.msm_checksum(k, scalars)
+
+
+@pytest.mark.parametrize("dist", ["uniform", "skewed"])
+@pytest.mark.parametrize("log_n", [12, 16, 18])
+def test_generated_bases(gpu, oracle, dist, log_n):
+    n = 1 << log_n
+    scalars, k = synth.workload(dist, n, 100 + log_n)
+    bd, _ = generated_bases(gpu, k)
+    res = gpu.msm(None, scalars, bases_dev=bd)
+    gpu.bc.free(bd)
+    assert oracle.horner(res) == oracle.msm_checksum(k, scalars)
+
+
+def test_generator_multiples_match_oracle(gpu, oracle):
+    k = synth.base_multipliers(77, 1024)
+    k[0] = 0
+    k[0, 0] = 1  # 1 * G
+    k[1] = H.limbs(H.R - 1)  # -G
+    _, host = generated_bases(gpu, k)
+    assert (host == oracle.gen_bases(k)).all()
+
+
+def test_edge_scalars(gpu, oracle):
+    table = H.load_g_bases()
+    n = 64
+    bases = H.mont_point_array([table[i % 256] for i in range(n)])
+    k = np.zeros((n, 8), np.uint32)
+    k[:, 0] = (np.arange(n) % 256) + 1
+    for values in ([0] * n, [1] * n, [H.R - 1] * n, [(H.R - 1) // 2] * n, [(H.R + 1) // 2] * n, [1 << 253] * n,
+                   [(1 << 16) + i for i in range(n)]):
+        scalars = H.mont_scalar_array(values)
+        assert oracle.horner(gpu.msm(bases, scalars)) == oracle.msm_checksum(k, scalars)
+
+
+def test_cancellation_and_repeats(gpu, oracle):
+    """s*P + (r-s)*P = 0 and many copies of one base in one bucket."""
+    table = H.load_g_bases()
+    bases = H.mont_point_array([table[3]] * 256)
+    vals = [7] * 128 + [H.R - 7] * 128
+    scalars = H.mont_scalar_array(vals)
+    assert oracle.horner(gpu.msm(bases, scalars))[0]
+    scalars = H.mont_scalar_array([5] * 256)
+    assert oracle.horner(gpu.msm(bases, scalars)) == oracle.affine_mul(1, 2, 4 * 5 * 256)
+
+
+@pytest.mark.parametrize("smem,rmem", [("device", "device"), ("pinned", "pinned"), ("pageable", "pageable"),
+                                        ("pinned", "device"), ("device", "pageable")])
+def test_memory_residence(gpu, oracle, smem, rmem):
+    """Scalars and results in device, pinned or pageable memory (msm_test.cu:172-260)."""
+    bases, scalars, k = H.table_workload(1 << 12, 3)
+    assert oracle.horner(gpu.msm(bases, scalars, scalars_mem=smem, results_mem=rmem)) == oracle.msm_checksum(k, scalars)
+
+
+def test_host_bases(gpu, oracle):
+    """Bases in pageable host memory are copied in, like the reference (src/msm.cu:175-182)."""
+    import bellman_cuda as bcm
+    bases, scalars, k = H.table_workload(1 << 10, 4)
+    res = np.zeros((254, 24), np.uint32)
+    gpu.bc.msm(gpu.pool, gpu.stream, np.ascontiguousarray(bases), np.ascontiguousarray(scalars), res, 10)
+    gpu.bc.stream_synchronize(gpu.stream)
+    assert oracle.horner(res) == oracle.msm_checksum(k, scalars)
+    del bcm
+
+
+def test_events_and_callbacks(gpu, oracle):
+    """h2d / d2h events are recorded and callbacks fire when copies happen."""
+    import bellman_cuda as bcm
+    bc = gpu.bc
+    bases, scalars, k = H.table_workload(1 << 11, 5)
+    bd = gpu.upload(bases)
+    fired = []
+    cb = bcm.HOST_FN(lambda data: fired.append(data))
+    e1, e2 = bc.event_create(), bc.event_create()
+    res = np.zeros((254, 24), np.uint32)
+    bc.msm(gpu.pool, gpu.stream, bd, np.ascontiguousarray(scalars), res, 11, h2d_event=e1, h2d_callback=cb, h2d_data=1,
+           d2h_event=e2, d2h_callback=cb, d2h_data=2)
+    bc.stream_synchronize(gpu.stream)
+    bc.event_synchronize(e1)
+    bc.event_synchronize(e2)
+    assert sorted(fired) == [1, 2]
+    assert oracle.horner(res) == oracle.msm_checksum(k, scalars)
+    bc.event_destroy(e1)
+    bc.event_destroy(e2)
+    bc.free(bd)
+
+
+def test_invalid_arguments(gpu):
+    bc = gpu.bc
+    res = np.zeros((254, 24), np.uint32)
+    assert bc.msm_execute_async(gpu.pool, gpu.stream, None, None, res, 4) == 1
+    assert bc.msm_execute_async(gpu.pool, gpu.stream, 16, 16, res, 40) == 1
+    assert bc.lib.ff_set_up(29, 14) == 1
+
+
+@pytest.mark.parametrize("window_bits", [2, 3, 5, 8, 11, 13, 16, 17, 20])
+def test_any_window_and_length(gpu, oracle, window_bits):
+    """The extension entry point: any length, forced window widths."""
+    n = 3001
+    bases, scalars, k = H.table_workload(n, 6)
+    bd, sd = gpu.upload(bases), gpu.upload(scalars)
+    rd = gpu.bc.malloc(254 * 96)
+    assert gpu.bc.msm_any(gpu.pool, gpu.stream, bd, sd, rd, n, window_bits) == 0
+    gpu.bc.stream_synchronize(gpu.stream)
+    res = gpu.bc.from_device(rd, (254, 24))
+    for p in (bd, sd, rd):
+        gpu.bc.free(p)
+    assert oracle.horner(res) == oracle.msm_checksum(k, scalars)
+
+
+@pytest.mark.parametrize("dist", ["uniform", "skewed"])
+def test_full_size_2_22(gpu, oracle, dist):
+    """Configs 1 and 2 (N = 2^22, seeds 1 and 2) against the checksum oracle."""
+    seed = 1 if dist == "uniform" else 2
+    n = 1 << 22
+    scalars, k = synth.workload(dist, n, seed)
+    bd, _ = generated_bases(gpu, k)
+    res = gpu.msm(None, scalars, bases_dev=bd)
+    gpu.bc.free(bd)
+    assert oracle.horner(res) == oracle.msm_checksum(k, scalars)
+
+
+# ---- the reference's own sm_100a build on identical inputs ----------------------
+@pytest.mark.parametrize("log_n", [0, 8, 12])
+def test_reference_parity_small(gpu, ref_gpu, oracle, log_n):
+    bases, scalars, k = H.table_workload(1 << log_n, 20 + log_n)
+    ours = oracle.horner(gpu.msm(bases, scalars))
+    theirs = oracle.horner(ref_gpu.msm(bases, scalars))
+    assert ours == theirs == oracle.msm_checksum(k, scalars)
+
+
+@pytest.mark.parametrize("dist", ["uniform", "skewed"])
+def test_reference_parity_2_22(gpu, ref_gpu, oracle, dist):
+    seed = 1 if dist == "uniform" else 2
+    n = 1 << 22
+    scalars, k = synth.workload(dist, n, seed)
+    bd, bases = generated_bases(gpu, k)
+    ours = oracle.horner(gpu.msm(None, scalars, bases_dev=bd))
+    gpu.bc.free(bd)
+    theirs = oracle.horner(ref_gpu.msm(bases, scalars))
+    assert ours == theirs

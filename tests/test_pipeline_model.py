@@ -1,0 +1,156 @@
+"""Integer model of the GPU pipeline's decomposition (a point is its discrete
+log mod r): signed digits of min(s, r - s), stable per-window sort, equal
+ranges with head partial sums, chunked head merging, grouped running sums and
+the binary decomposition that places every partial sum at its bit of the
+254-entry result.  Checks sum_i 2^i R_i == sum_i k_i s_i, and that no partial
+sum lands above bit 253.  Mirrors era-bellman-cuda_b200/csrc/msm_kernels.cu."""
+import random
+
+import pytest
+
+R = 0x30644E72E131A029B85045B68181585D2833E84879B9709143E1F593F0000001
+
+
+def model_msm(scal, kl, c, T, chunk=4, log_m_max=4):
+    n = len(scal)
+    W = (254 + c - 1) // c
+    log_b = c - 1
+    B = 1 << log_b
+    keys = [[0] * n for _ in range(W)]
+    vals = [[None] * n for _ in range(W)]
+    for i, s in enumerate(scal):
+        neg = R - s
+        flip = neg < s
+        if flip:
+            s = neg
+        assert s < (1 << 253)
+        carry = 0
+        for w in range(W):
+            raw = ((s >> (w * c)) & ((1 << c) - 1)) + carry
+            negd = 0
+            if raw > B:
+                raw, negd, carry = (1 << c) - raw, 1, 1
+            else:
+                carry = 0
+            keys[w][i], vals[w][i] = raw, (i, negd ^ flip)
+        assert carry == 0
+    for w in range(W):
+        order = sorted(range(n), key=lambda i: keys[w][i])
+        keys[w] = [keys[w][i] for i in order]
+        vals[w] = [vals[w][i] for i in order]
+    zeros = [sum(1 for k in keys[w] if k == 0) for w in range(W)]
+    pre = [0]
+    for w in range(W):
+        pre.append(pre[-1] + n - zeros[w])
+    M = pre[-1]
+
+    def entry(v):
+        w = next(x for x in range(W) if pre[x] <= v < pre[x + 1])
+        return w, zeros[w] + v - pre[w]
+
+    def point(w, idx):
+        i, sg = vals[w][idx]
+        return (-kl[i] if sg else kl[i]) % R
+
+    buckets, hb, hp = {}, [None] * T, [0] * T
+    for t in range(T):
+        beg, end = M * t // T, M * (t + 1) // T
+        if beg == end:
+            continue
+        w, idx = entry(beg)
+        key = keys[w][idx]
+        cont = idx > zeros[w] and keys[w][idx - 1] == key
+        cur, acc, first = (w << log_b) | (key & (B - 1)), point(w, idx), True
+        for v in range(beg + 1, end):
+            w, idx = entry(v)
+            b = (w << log_b) | (keys[w][idx] & (B - 1))
+            if b != cur:
+                if first and cont:
+                    hb[t], hp[t] = cur, acc
+                else:
+                    assert cur not in buckets
+                    buckets[cur] = acc
+                first, cur, acc = False, b, point(w, idx)
+            else:
+                acc = (acc + point(w, idx)) % R
+        if first and cont:
+            hb[t], hp[t] = cur, acc
+        else:
+            assert cur not in buckets
+            buckets[cur] = acc
+    heads = T
+    while heads > 1:
+        out = (heads + chunk - 1) // chunk
+        hb2, hp2 = [None] * out, [0] * out
+        for u in range(out):
+            beg, end = u * chunk, min(heads, u * chunk + chunk)
+            bucket, isc, seen, acc = None, False, False, 0
+            for k in range(beg, end):
+                b = hb[k]
+                if b is None:
+                    continue
+                if b != bucket:
+                    if bucket is not None:
+                        if isc:
+                            hb2[u], hp2[u] = bucket, acc
+                        else:
+                            buckets[bucket] = (buckets[bucket] + acc) % R
+                    isc = (not seen) and k == beg and k > 0 and hb[k - 1] == b
+                    seen, bucket, acc = True, b, hp[k]
+                else:
+                    acc = (acc + hp[k]) % R
+            if bucket is not None:
+                if isc:
+                    hb2[u], hp2[u] = bucket, acc
+                else:
+                    buckets[bucket] = (buckets[bucket] + acc) % R
+        hb, hp, heads = hb2, hp2, out
+    log_m = min(log_m_max, log_b)
+    log_g = log_b - log_m
+    G, m = 1 << log_g, 1 << log_m
+    res = [0] * 254
+    for w in range(W):
+        run, accs = [0] * G, [0] * G
+        for g in range(G):
+            r_, a_ = 0, 0
+            for i in range(m - 1, 0, -1):
+                r_ = (r_ + buckets.get((w << log_b) + g * m + i, 0)) % R
+                a_ = (a_ + r_) % R
+            if g > 0:
+                r_ = (r_ + buckets.get((w << log_b) + g * m, 0)) % R
+            run[g], accs[g] = r_, a_
+        streams, t0 = [accs], run
+        for _ in range(log_g):
+            streams.append(t0[1::2])
+            t0 = [(t0[2 * i] + t0[2 * i + 1]) % R for i in range(len(t0) // 2)]
+        sums = [sum(s) % R for s in streams]
+        for o in range(c):
+            val = 0
+            if o == 0:
+                val = sums[0]
+            elif o == c - 1:
+                val = buckets.get(w << log_b, 0)
+            elif log_m <= o < log_m + log_g:
+                val = sums[o - log_m + 1]
+            if c * w + o >= 254:
+                assert val == 0
+            else:
+                res[c * w + o] = val
+    return sum(res[i] * pow(2, i, R) for i in range(254)) % R
+
+
+@pytest.mark.parametrize("trial", range(24))
+def test_model_matches_sum(trial):
+    rng = random.Random(trial)
+    n = rng.choice([1, 2, 3, 5, 16, 33, 100, 257])
+    c = rng.choice([2, 3, 4, 5, 6, 8, 10, 12, 16])
+    T = rng.choice([1, 2, 3, 7, 16, 64, 200])
+    mode = rng.choice(["uniform", "small", "skewed"])
+    if mode == "uniform":
+        scal = [rng.randrange(R) for _ in range(n)]
+    elif mode == "small":
+        scal = [rng.choice([0, 1, 2, R - 1, R - 2, rng.randrange(1 << 16)]) for _ in range(n)]
+    else:
+        scal = [rng.choice([0, 0, 1, 1, rng.randrange(1 << 16), rng.randrange(R)]) for _ in range(n)]
+    kl = [rng.randrange(1, R) for _ in range(n)]
+    assert model_msm(scal, kl, c, T) == sum(s * k for s, k in zip(scal, kl)) % R
