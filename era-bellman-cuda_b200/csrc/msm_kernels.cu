@@ -320,12 +320,17 @@ __global__ void __launch_bounds__(ACC_THREADS) accumulate_kernel(const uint32_t 
   const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= total_threads)
     return;
+  // Only the first min(total, total_threads) ranges are used, so every active
+  // range holds at least one entry and the heads of one bucket stay
+  // contiguous (an empty range between them would let two merge threads
+  // update the same bucket).
   const unsigned long long total = s_prefix[windows];
-  const unsigned long long beg = total * t / total_threads;
-  const unsigned long long end = total * (t + 1) / total_threads;
+  const unsigned long long active = total < total_threads ? total : total_threads;
   head_bucket[t] = INVALID_BUCKET;
-  if (beg == end)
+  if (t >= active)
     return;
+  const unsigned long long beg = total * t / active;
+  const unsigned long long end = total * (t + 1) / active;
   unsigned w = 0;
   while (w + 1 < windows && s_prefix[w + 1] <= beg)
     w++;

@@ -53,10 +53,10 @@ def model_msm(scal, kl, c, T, chunk=4, log_m_max=4):
         return (-kl[i] if sg else kl[i]) % R
 
     buckets, hb, hp = {}, [None] * T, [0] * T
-    for t in range(T):
-        beg, end = M * t // T, M * (t + 1) // T
-        if beg == end:
-            continue
+    active = min(M, T)
+    for t in range(active):
+        beg, end = M * t // active, M * (t + 1) // active
+        assert beg < end
         w, idx = entry(beg)
         key = keys[w][idx]
         cont = idx > zeros[w] and keys[w][idx - 1] == key
@@ -80,8 +80,15 @@ def model_msm(scal, kl, c, T, chunk=4, log_m_max=4):
             buckets[cur] = acc
     heads = T
     while heads > 1:
+        # the heads of one bucket must be contiguous: one merge launch may not
+        # update a bucket from two threads
+        valid = [k for k in range(heads) if hb[k] is not None]
+        for a, b in zip(valid, valid[1:]):
+            if hb[a] == hb[b]:
+                assert b == a + 1, "heads of one bucket are not contiguous"
         out = (heads + chunk - 1) // chunk
         hb2, hp2 = [None] * out, [0] * out
+        updated = set()
         for u in range(out):
             beg, end = u * chunk, min(heads, u * chunk + chunk)
             bucket, isc, seen, acc = None, False, False, 0
@@ -94,6 +101,8 @@ def model_msm(scal, kl, c, T, chunk=4, log_m_max=4):
                         if isc:
                             hb2[u], hp2[u] = bucket, acc
                         else:
+                            assert bucket not in updated
+                            updated.add(bucket)
                             buckets[bucket] = (buckets[bucket] + acc) % R
                     isc = (not seen) and k == beg and k > 0 and hb[k - 1] == b
                     seen, bucket, acc = True, b, hp[k]
@@ -103,6 +112,8 @@ def model_msm(scal, kl, c, T, chunk=4, log_m_max=4):
                 if isc:
                     hb2[u], hp2[u] = bucket, acc
                 else:
+                    assert bucket not in updated
+                    updated.add(bucket)
                     buckets[bucket] = (buckets[bucket] + acc) % R
         hb, hp, heads = hb2, hp2, out
     log_m = min(log_m_max, log_b)
@@ -139,7 +150,7 @@ def model_msm(scal, kl, c, T, chunk=4, log_m_max=4):
     return sum(res[i] * pow(2, i, R) for i in range(254)) % R
 
 
-@pytest.mark.parametrize("trial", range(24))
+@pytest.mark.parametrize("trial", range(40))
 def test_model_matches_sum(trial):
     rng = random.Random(trial)
     n = rng.choice([1, 2, 3, 5, 16, 33, 100, 257])
