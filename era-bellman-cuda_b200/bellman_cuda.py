@@ -18,6 +18,8 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_LIBRARY = os.path.join(HERE, "lib", "libbellman_cuda_b200.so")
+# BCB200_LIBRARY points the binding at another build of the same sources (experiments)
+DEFAULT_LIBRARY = os.environ.get("BCB200_LIBRARY", DEFAULT_LIBRARY)
 
 RESULT_BITS = 254
 FE_BYTES = 32

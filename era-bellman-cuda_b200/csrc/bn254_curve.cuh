@@ -57,7 +57,7 @@ struct curve {
 
   // 2 * a for an affine a (mdbl-2008-s-1): U = 2Y, V = U^2, W = U V,
   // S = X V, M = 3 X^2, X3 = M^2 - 2S, Y3 = M (S - X3) - W Y, ZZ3 = V, ZZZ3 = W.
-  static BN_HD xyzz dbl_affine(const affine &a) {
+  static BN_HD_COLD xyzz dbl_affine(const affine &a) {
     const fe U = fq::dbl(a.y);
     const fe V = fq::sqr(U);
     const fe W = fq::mul(U, V);
@@ -73,7 +73,7 @@ struct curve {
   }
 
   // 2 * p (dbl-2008-s-1): as above with ZZ3 = V ZZ1, ZZZ3 = W ZZZ1.
-  static BN_HD xyzz dbl(const xyzz &p) {
+  static BN_HD_COLD xyzz dbl(const xyzz &p) {
     if (is_inf(p))
       return p;
     const fe U = fq::dbl(p.y);
@@ -106,6 +106,31 @@ struct curve {
       if (fq::is_zero(R))
         return dbl_affine(a); // p == a
       return infinity();      // p == -a
+    }
+    const fe PP = fq::sqr(P);
+    const fe PPP = fq::mul(P, PP);
+    const fe Q = fq::mul(p.x, PP);
+    xyzz r;
+    r.x = fq::sub(fq::sub(fq::sqr(R), PPP), fq::dbl(Q));
+    r.y = fq::mul_sub_mul(R, fq::sub(Q, r.x), p.y, PPP);
+    r.zz = fq::mul(p.zz, PP);
+    r.zzz = fq::mul(p.zzz, PPP);
+    return r;
+  }
+
+  // p + a for a finite accumulator p (no test of p's ZZ): the accumulation
+  // loop tracks infinity itself.  Sets became_inf when the sum is infinity
+  // (p == -a); the returned point is then unspecified.
+  static BN_HD xyzz add_affine_finite(const xyzz &p, const affine &a, bool &became_inf) {
+    const fe U2 = fq::mul(a.x, p.zz);
+    const fe S2 = fq::mul(a.y, p.zzz);
+    const fe P = fq::sub(U2, p.x);
+    const fe R = fq::sub(S2, p.y);
+    if (fq::is_zero(P)) {
+      if (fq::is_zero(R))
+        return dbl_affine(a); // p == a
+      became_inf = true;      // p == -a
+      return p;
     }
     const fe PP = fq::sqr(P);
     const fe PPP = fq::mul(P, PP);

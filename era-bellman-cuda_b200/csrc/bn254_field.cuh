@@ -23,10 +23,20 @@
 #define BN_HD __host__ __device__ __forceinline__
 #define BN_DEV __device__ __forceinline__
 #define BN_ALIGN(n) __align__(n)
+// rarely taken paths (point doubling inside an addition) stay out of line so
+// the hot loop's instructions fit the instruction cache
+#define BN_HD_COLD __host__ __device__ __noinline__
+#if defined(BN254_OUTLINE_MUL)
+#define BN_HD_MUL __host__ __device__ __noinline__
+#else
+#define BN_HD_MUL __host__ __device__ __forceinline__
+#endif
 #else
 #define BN_HD inline
 #define BN_DEV inline
 #define BN_ALIGN(n) alignas(n)
+#define BN_HD_COLD inline
+#define BN_HD_MUL inline
 #endif
 
 namespace bn254 {
@@ -319,6 +329,18 @@ template <class F> struct field {
 
   static BN_HD fe neg(const fe &a) { return sub(zero(), a); }
 
+  // 2m - a for a in (0, 2m): the negation of a nonzero value as a lazy value
+  // in (0, 2m), one borrow chain
+  static BN_HD fe neg_nonzero(const fe &a) {
+    fe r;
+    r.l[0] = cc::sub_cc(F::mod2(0), a.l[0]);
+#pragma unroll
+    for (int i = 1; i < 7; i++)
+      r.l[i] = cc::subc_cc(F::mod2(i), a.l[i]);
+    r.l[7] = cc::subc(F::mod2(7), a.l[7]);
+    return r;
+  }
+
   // [0, 2m) -> [0, m)
   static BN_HD fe reduce_full(const fe &a) {
     fe d;
@@ -352,189 +374,269 @@ template <class F> struct field {
     return z == 0 || m == 0;
   }
 
-  // ---- Montgomery multiplication (CIOS, one operand word per round) -------
-  // Round i: T += a*b[i]  (low halves into words 0..7, high halves into 1..8),
-  //          q = T[0]*INV,  T += q*m  (same two chains),  T >>= 32.
-  // T < 2m*2^32 + 2m + m*2^32 < 2^288 during a round, so nine words hold it
-  // and the last instruction of each high-half chain has no carry out.
-  // 33 multiply instructions per round, 264 in total; inputs < 2m give an
+  // ---- Montgomery multiplication -------------------------------------------
+  // CIOS, one operand word per round.  T is held in two accumulators whose
+  // words are used in fixed (low, high) pairs, so that the two halves of each
+  // 32 x 32 product are adjacent in one carry chain and every pair keeps its
+  // partner across rounds (a pair that changed partners would cost register
+  // moves):
+  //   the "even" accumulator takes products at word positions (0,1) (2,3)
+  //   (4,5) (6,7) -- the even limbs x[0,2,4,6] times y, and q * m[0,2,4,6];
+  //   the "odd" accumulator takes (1,2) (3,4) (5,6) (7,8) -- the odd limbs.
+  // Dividing T by 2^32 moves every word down one position, which turns the
+  // odd accumulator's pairs into even-aligned pairs and vice versa, so the
+  // two arrays simply swap roles each round; array index = position + round.
+  // The one word left unpaired (the old even accumulator's word at the new
+  // position 0) is folded into the new even accumulator at the start of the
+  // next round; its carry enters the odd chain, which starts at position 1.
+  // During a round T < 4m + 3m * 2^32 < 2^288 and each accumulator is <= T,
+  // so nine words hold either one and odd chains never carry out of their
+  // last word.  33 multiply instructions per round; inputs < 2m give an
   // output < 2m.
-  static BN_HD fe mul(const fe &a, const fe &b) {
-    uint32_t t0, t1, t2, t3, t4, t5, t6, t7, t8;
-    // round 0: T = a*b[0] + q*m with T starting at zero
-    {
-      const uint32_t bi = b.l[0];
-      t0 = cc::mul_lo(a.l[0], bi);
-      t1 = cc::mul_lo(a.l[1], bi);
-      t2 = cc::mul_lo(a.l[2], bi);
-      t3 = cc::mul_lo(a.l[3], bi);
-      t4 = cc::mul_lo(a.l[4], bi);
-      t5 = cc::mul_lo(a.l[5], bi);
-      t6 = cc::mul_lo(a.l[6], bi);
-      t7 = cc::mul_lo(a.l[7], bi);
-      t1 = cc::mad_hi_cc(a.l[0], bi, t1);
-      t2 = cc::madc_hi_cc(a.l[1], bi, t2);
-      t3 = cc::madc_hi_cc(a.l[2], bi, t3);
-      t4 = cc::madc_hi_cc(a.l[3], bi, t4);
-      t5 = cc::madc_hi_cc(a.l[4], bi, t5);
-      t6 = cc::madc_hi_cc(a.l[5], bi, t6);
-      t7 = cc::madc_hi_cc(a.l[6], bi, t7);
-      t8 = cc::madc_hi(a.l[7], bi, 0);
-      reduce_round(t0, t1, t2, t3, t4, t5, t6, t7, t8);
-    }
-#pragma unroll
-    for (int i = 1; i < 8; i++) {
-      const uint32_t bi = b.l[i];
-      // t0..t7 hold T (< 2m), t8 == 0
-      t0 = cc::mad_lo_cc(a.l[0], bi, t0);
-      t1 = cc::madc_lo_cc(a.l[1], bi, t1);
-      t2 = cc::madc_lo_cc(a.l[2], bi, t2);
-      t3 = cc::madc_lo_cc(a.l[3], bi, t3);
-      t4 = cc::madc_lo_cc(a.l[4], bi, t4);
-      t5 = cc::madc_lo_cc(a.l[5], bi, t5);
-      t6 = cc::madc_lo_cc(a.l[6], bi, t6);
-      t7 = cc::madc_lo_cc(a.l[7], bi, t7);
-      t8 = cc::addc(0, 0);
-      t1 = cc::mad_hi_cc(a.l[0], bi, t1);
-      t2 = cc::madc_hi_cc(a.l[1], bi, t2);
-      t3 = cc::madc_hi_cc(a.l[2], bi, t3);
-      t4 = cc::madc_hi_cc(a.l[3], bi, t4);
-      t5 = cc::madc_hi_cc(a.l[4], bi, t5);
-      t6 = cc::madc_hi_cc(a.l[5], bi, t6);
-      t7 = cc::madc_hi_cc(a.l[6], bi, t7);
-      t8 = cc::madc_hi(a.l[7], bi, t8);
-      reduce_round(t0, t1, t2, t3, t4, t5, t6, t7, t8);
-    }
+
+  // A[R..R+7] += x[0,2,4,6] * y; carry into A[R+8] (fresh word)
+  template <int R> static BN_HD void even_products(uint32_t *A, const uint32_t *x, uint32_t y) {
+    A[R + 0] = cc::mad_lo_cc(x[0], y, A[R + 0]);
+    A[R + 1] = cc::madc_hi_cc(x[0], y, A[R + 1]);
+    A[R + 2] = cc::madc_lo_cc(x[2], y, A[R + 2]);
+    A[R + 3] = cc::madc_hi_cc(x[2], y, A[R + 3]);
+    A[R + 4] = cc::madc_lo_cc(x[4], y, A[R + 4]);
+    A[R + 5] = cc::madc_hi_cc(x[4], y, A[R + 5]);
+    A[R + 6] = cc::madc_lo_cc(x[6], y, A[R + 6]);
+    A[R + 7] = cc::madc_hi_cc(x[6], y, A[R + 7]);
+    A[R + 8] = cc::addc(A[R + 8], 0);
+  }
+
+  // B[R+1..R+8] += x[1,3,5,7] * y, no carry out; CARRY_IN consumes the flag
+  template <int R, bool CARRY_IN> static BN_HD void odd_products(uint32_t *B, const uint32_t *x, uint32_t y) {
+    B[R + 1] = CARRY_IN ? cc::madc_lo_cc(x[1], y, B[R + 1]) : cc::mad_lo_cc(x[1], y, B[R + 1]);
+    B[R + 2] = cc::madc_hi_cc(x[1], y, B[R + 2]);
+    B[R + 3] = cc::madc_lo_cc(x[3], y, B[R + 3]);
+    B[R + 4] = cc::madc_hi_cc(x[3], y, B[R + 4]);
+    B[R + 5] = cc::madc_lo_cc(x[5], y, B[R + 5]);
+    B[R + 6] = cc::madc_hi_cc(x[5], y, B[R + 6]);
+    B[R + 7] = cc::madc_lo_cc(x[7], y, B[R + 7]);
+    B[R + 8] = cc::madc_hi(x[7], y, B[R + 8]);
+  }
+
+  // the same two chains against the modulus
+  template <int R> static BN_HD void even_reduce(uint32_t *A, uint32_t q) {
+    A[R + 0] = cc::mad_lo_cc(q, F::mod(0), A[R + 0]); // becomes 0; the carry matters
+    A[R + 1] = cc::madc_hi_cc(q, F::mod(0), A[R + 1]);
+    A[R + 2] = cc::madc_lo_cc(q, F::mod(2), A[R + 2]);
+    A[R + 3] = cc::madc_hi_cc(q, F::mod(2), A[R + 3]);
+    A[R + 4] = cc::madc_lo_cc(q, F::mod(4), A[R + 4]);
+    A[R + 5] = cc::madc_hi_cc(q, F::mod(4), A[R + 5]);
+    A[R + 6] = cc::madc_lo_cc(q, F::mod(6), A[R + 6]);
+    A[R + 7] = cc::madc_hi_cc(q, F::mod(6), A[R + 7]);
+    A[R + 8] = cc::addc(A[R + 8], 0);
+  }
+
+  template <int R, bool CARRY_IN> static BN_HD void odd_reduce(uint32_t *B, uint32_t q) {
+    B[R + 1] = CARRY_IN ? cc::madc_lo_cc(q, F::mod(1), B[R + 1]) : cc::mad_lo_cc(q, F::mod(1), B[R + 1]);
+    B[R + 2] = cc::madc_hi_cc(q, F::mod(1), B[R + 2]);
+    B[R + 3] = cc::madc_lo_cc(q, F::mod(3), B[R + 3]);
+    B[R + 4] = cc::madc_hi_cc(q, F::mod(3), B[R + 4]);
+    B[R + 5] = cc::madc_lo_cc(q, F::mod(5), B[R + 5]);
+    B[R + 6] = cc::madc_hi_cc(q, F::mod(5), B[R + 6]);
+    B[R + 7] = cc::madc_lo_cc(q, F::mod(7), B[R + 7]);
+    B[R + 8] = cc::madc_hi(q, F::mod(7), B[R + 8]);
+  }
+
+  // Round R >= 1 of the product (A = even role, B = odd role this round).
+  template <int R> static BN_HD void mul_round(uint32_t *A, uint32_t *B, const uint32_t *x, uint32_t y) {
+    A[R] = cc::add_cc(A[R], B[R]); // fold B's unpaired word; the carry belongs to position 1
+    odd_products<R, true>(B, x, y);
+    even_products<R>(A, x, y);
+    const uint32_t q = cc::mul_lo(A[R], F::INV);
+    even_reduce<R>(A, q);
+    odd_reduce<R, false>(B, q);
+  }
+
+  // Round R >= 1 of a reduction without products.
+  template <int R> static BN_HD void redc_round(uint32_t *A, uint32_t *B) {
+    A[R] = cc::add_cc(A[R], B[R]);
+    const uint32_t q = cc::mul_lo(A[R], F::INV);
+    odd_reduce<R, true>(B, q);
+    even_reduce<R>(A, q);
+  }
+
+  // result positions 0..7 live at index 8 of both arrays after eight rounds
+  static BN_HD fe merge8(const uint32_t *X, const uint32_t *Y) {
     fe r;
-    r.l[0] = t0;
-    r.l[1] = t1;
-    r.l[2] = t2;
-    r.l[3] = t3;
-    r.l[4] = t4;
-    r.l[5] = t5;
-    r.l[6] = t6;
-    r.l[7] = t7;
+    r.l[0] = cc::add_cc(X[8], Y[8]);
+#pragma unroll
+    for (int k = 1; k < 7; k++)
+      r.l[k] = cc::addc_cc(X[8 + k], Y[8 + k]);
+    r.l[7] = cc::addc(X[15], Y[15]);
     return r;
   }
 
-  // One reduction round on the nine-word window t0..t8:
-  //   q = t0*INV; (t0..t8) += q*m; shift down one word (t8 becomes 0).
-  static BN_HD void reduce_round(uint32_t &t0, uint32_t &t1, uint32_t &t2, uint32_t &t3, uint32_t &t4, uint32_t &t5, uint32_t &t6,
-                                 uint32_t &t7, uint32_t &t8) {
-    const uint32_t q = cc::mul_lo(t0, F::INV);
-    t0 = cc::mad_lo_cc(q, F::mod(0), t0); // == 0, only the carry matters
-    t1 = cc::madc_lo_cc(q, F::mod(1), t1);
-    t2 = cc::madc_lo_cc(q, F::mod(2), t2);
-    t3 = cc::madc_lo_cc(q, F::mod(3), t3);
-    t4 = cc::madc_lo_cc(q, F::mod(4), t4);
-    t5 = cc::madc_lo_cc(q, F::mod(5), t5);
-    t6 = cc::madc_lo_cc(q, F::mod(6), t6);
-    t7 = cc::madc_lo_cc(q, F::mod(7), t7);
-    t8 = cc::addc(t8, 0);
-    t1 = cc::mad_hi_cc(q, F::mod(0), t1);
-    t2 = cc::madc_hi_cc(q, F::mod(1), t2);
-    t3 = cc::madc_hi_cc(q, F::mod(2), t3);
-    t4 = cc::madc_hi_cc(q, F::mod(3), t4);
-    t5 = cc::madc_hi_cc(q, F::mod(4), t5);
-    t6 = cc::madc_hi_cc(q, F::mod(5), t6);
-    t7 = cc::madc_hi_cc(q, F::mod(6), t7);
-    t8 = cc::madc_hi(q, F::mod(7), t8);
-    t0 = t1;
-    t1 = t2;
-    t2 = t3;
-    t3 = t4;
-    t4 = t5;
-    t5 = t6;
-    t6 = t7;
-    t7 = t8;
-    t8 = 0;
+  static BN_HD_MUL fe mul(const fe &a, const fe &b) {
+    uint32_t X[17], Y[17];
+#pragma unroll
+    for (int k = 0; k < 17; k++) {
+      X[k] = 0;
+      Y[k] = 0;
+    }
+    {
+      // round 0 on T = 0: products land in empty words (X even role, Y odd)
+      const uint32_t y = b.l[0];
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        X[2 * k] = cc::mul_lo(a.l[2 * k], y);
+        X[2 * k + 1] = cc::mul_hi(a.l[2 * k], y);
+        Y[2 * k + 1] = cc::mul_lo(a.l[2 * k + 1], y);
+        Y[2 * k + 2] = cc::mul_hi(a.l[2 * k + 1], y);
+      }
+      const uint32_t q = cc::mul_lo(X[0], F::INV);
+      even_reduce<0>(X, q);
+      odd_reduce<0, false>(Y, q);
+    }
+    mul_round<1>(Y, X, a.l, b.l[1]);
+    mul_round<2>(X, Y, a.l, b.l[2]);
+    mul_round<3>(Y, X, a.l, b.l[3]);
+    mul_round<4>(X, Y, a.l, b.l[4]);
+    mul_round<5>(Y, X, a.l, b.l[5]);
+    mul_round<6>(X, Y, a.l, b.l[6]);
+    mul_round<7>(Y, X, a.l, b.l[7]);
+    return merge8(X, Y);
   }
 
-  // Full 512-bit product (128 multiply instructions).  Row i adds a*b[i] at
-  // word i; after row i the partial product is < 2^(32(i+9)), so the high
-  // chain of row i never carries past word i+8.
-  static BN_HD fe_wide mul_wide(const fe &a, const fe &b) {
-    fe_wide w;
+  // Montgomery reduction of a 256-bit value: eight rounds of q*m only.
+  // Returns REDC(x) = x * 2^-256 mod m in [0, m] (x + q*m < 2^256 (1 + m)).
+  static BN_HD fe redc_low(const fe &x) {
+    uint32_t X[17], Y[17];
+#pragma unroll
+    for (int k = 0; k < 17; k++) {
+      X[k] = k < 8 ? x.l[k < 8 ? k : 0] : 0;
+      Y[k] = 0;
+    }
     {
-      const uint32_t b0 = b.l[0];
-#pragma unroll
-      for (int j = 0; j < 8; j++)
-        w.l[j] = cc::mul_lo(a.l[j], b0);
-      w.l[1] = cc::mad_hi_cc(a.l[0], b0, w.l[1]);
-#pragma unroll
-      for (int j = 1; j < 7; j++)
-        w.l[j + 1] = cc::madc_hi_cc(a.l[j], b0, w.l[j + 1]);
-      w.l[8] = cc::madc_hi(a.l[7], b0, 0);
+      const uint32_t q = cc::mul_lo(X[0], F::INV);
+      even_reduce<0>(X, q);
+      odd_reduce<0, false>(Y, q);
     }
+    redc_round<1>(Y, X);
+    redc_round<2>(X, Y);
+    redc_round<3>(Y, X);
+    redc_round<4>(X, Y);
+    redc_round<5>(Y, X);
+    redc_round<6>(X, Y);
+    redc_round<7>(Y, X);
+    return merge8(X, Y);
+  }
+
+  // Full 512-bit product a*b (128 multiply instructions).  A product
+  // a[j]*b[i] lands at word position i + j: E collects the even positions
+  // (pairs (2k, 2k+1)), O the odd ones (pairs (2k+1, 2k+2)), so pairs never
+  // change partners between rows.  Row i's partial sum is < 2^(32(i+9)):
+  // the chain that ends at word i+7 carries into a fresh word i+8, the one
+  // that ends at word i+8 never carries out.
+  static BN_HD fe_wide mul_wide(const fe &a, const fe &b) {
+    uint32_t E[17], O[17];
 #pragma unroll
-    for (int i = 1; i < 8; i++) {
-      const uint32_t bi = b.l[i];
-      w.l[i] = cc::mad_lo_cc(a.l[0], bi, w.l[i]);
-#pragma unroll
-      for (int j = 1; j < 8; j++)
-        w.l[i + j] = cc::madc_lo_cc(a.l[j], bi, w.l[i + j]);
-      w.l[i + 8] = cc::addc(0, 0);
-      w.l[i + 1] = cc::mad_hi_cc(a.l[0], bi, w.l[i + 1]);
-#pragma unroll
-      for (int j = 1; j < 7; j++)
-        w.l[i + j + 1] = cc::madc_hi_cc(a.l[j], bi, w.l[i + j + 1]);
-      w.l[i + 8] = cc::madc_hi(a.l[7], bi, w.l[i + 8]);
+    for (int k = 0; k < 17; k++) {
+      E[k] = 0;
+      O[k] = 0;
     }
+    {
+      const uint32_t y = b.l[0];
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        E[2 * k] = cc::mul_lo(a.l[2 * k], y);
+        E[2 * k + 1] = cc::mul_hi(a.l[2 * k], y);
+        O[2 * k + 1] = cc::mul_lo(a.l[2 * k + 1], y);
+        O[2 * k + 2] = cc::mul_hi(a.l[2 * k + 1], y);
+      }
+    }
+    wide_row<1>(E, O, a.l, b.l[1]);
+    wide_row<2>(E, O, a.l, b.l[2]);
+    wide_row<3>(E, O, a.l, b.l[3]);
+    wide_row<4>(E, O, a.l, b.l[4]);
+    wide_row<5>(E, O, a.l, b.l[5]);
+    wide_row<6>(E, O, a.l, b.l[6]);
+    wide_row<7>(E, O, a.l, b.l[7]);
+    fe_wide w;
+    w.l[0] = cc::add_cc(E[0], O[0]);
+#pragma unroll
+    for (int k = 1; k < 15; k++)
+      w.l[k] = cc::addc_cc(E[k], O[k]);
+    w.l[15] = cc::addc(E[15], O[15]);
     return w;
   }
 
-  // 512-bit square: off-diagonal products once (56 instructions), doubled,
-  // plus the diagonal (16 instructions).  Row i adds a[i]*a[j>i] at word i+j.
+  // row I >= 1 of mul_wide: even I puts even limbs at even positions (E) and
+  // odd limbs at odd positions (O); odd I the other way round
+  template <int I> static BN_HD void wide_row(uint32_t *E, uint32_t *O, const uint32_t *x, uint32_t y) {
+    if (I % 2 == 0) {
+      even_products<I>(E, x, y);        // E[I..I+7], carry into E[I+8]
+      odd_products<I, false>(O, x, y);  // O[I+1..I+8]
+    } else {
+      even_products<I>(O, x, y);        // x[0,2,4,6] at odd positions I..I+7, carry into O[I+8]
+      odd_products<I, false>(E, x, y);  // x[1,3,5,7] at even positions I+1..I+8
+    }
+  }
+
+  // 512-bit square: off-diagonal products a[i]*a[j] (i < j, 56 instructions)
+  // split by the parity of i + j so every chain pairs low and high halves,
+  // doubled, plus the diagonal a[i]^2 (16 instructions).  A chain of row i
+  // ends at most at word i + 8 and its carry goes to a word no earlier row
+  // has written.
   static BN_HD fe_wide sqr_wide(const fe &a) {
-    fe_wide w;
-    w.l[0] = 0;
-    // row 0: a0 * a1..a7 at words 1..8
-    {
-      const uint32_t ai = a.l[0];
+    uint32_t E[16], O[16];
 #pragma unroll
-      for (int j = 1; j < 8; j++)
-        w.l[j] = cc::mul_lo(ai, a.l[j]);
-      w.l[2] = cc::mad_hi_cc(ai, a.l[1], w.l[2]);
-#pragma unroll
-      for (int j = 2; j < 7; j++)
-        w.l[j + 1] = cc::madc_hi_cc(ai, a.l[j], w.l[j + 1]);
-      w.l[8] = cc::madc_hi(ai, a.l[7], 0);
+    for (int k = 0; k < 16; k++) {
+      E[k] = 0;
+      O[k] = 0;
     }
 #pragma unroll
-    for (int i = 1; i < 7; i++) {
-      const uint32_t ai = a.l[i];
-      // low halves of a[i]*a[j], j = i+1..7, at words 2i+1 .. i+7
-      w.l[2 * i + 1] = cc::mad_lo_cc(ai, a.l[i + 1], w.l[2 * i + 1]);
+    for (int i = 0; i < 7; i++) {
+      const uint32_t x = a.l[i];
+      // i + j odd: j = i+1, i+3, ... -> O
+      O[2 * i + 1] = cc::mad_lo_cc(x, a.l[i + 1], O[2 * i + 1]);
+      O[2 * i + 2] = cc::madc_hi_cc(x, a.l[i + 1], O[2 * i + 2]);
 #pragma unroll
-      for (int j = i + 2; j < 8; j++)
-        w.l[i + j] = cc::madc_lo_cc(ai, a.l[j], w.l[i + j]);
-      w.l[i + 8] = cc::addc(0, 0);
-      // high halves at words 2i+2 .. i+8
-      if (i + 1 < 7) {
-        w.l[2 * i + 2] = cc::mad_hi_cc(ai, a.l[i + 1], w.l[2 * i + 2]);
+      for (int j = i + 3; j < 8; j += 2) {
+        O[i + j] = cc::madc_lo_cc(x, a.l[j], O[i + j]);
+        O[i + j + 1] = cc::madc_hi_cc(x, a.l[j], O[i + j + 1]);
+      }
+      {
+        const int last = i + 1 + 2 * ((7 - (i + 1)) / 2); // largest j of that parity
+        O[i + last + 2] = cc::addc(O[i + last + 2], 0);
+      }
+      // i + j even: j = i+2, i+4, ... -> E
+      if (i + 2 < 8) {
+        E[2 * i + 2] = cc::mad_lo_cc(x, a.l[i + 2], E[2 * i + 2]);
+        E[2 * i + 3] = cc::madc_hi_cc(x, a.l[i + 2], E[2 * i + 3]);
 #pragma unroll
-        for (int j = i + 2; j < 7; j++)
-          w.l[i + j + 1] = cc::madc_hi_cc(ai, a.l[j], w.l[i + j + 1]);
-        w.l[i + 8] = cc::madc_hi(ai, a.l[7], w.l[i + 8]);
-      } else {
-        // i == 6: the single product a6*a7
-        w.l[14] = cc::mad_hi_cc(ai, a.l[7], w.l[14]);
+        for (int j = i + 4; j < 8; j += 2) {
+          E[i + j] = cc::madc_lo_cc(x, a.l[j], E[i + j]);
+          E[i + j + 1] = cc::madc_hi_cc(x, a.l[j], E[i + j + 1]);
+        }
+        const int last = i + 2 + 2 * ((7 - (i + 2)) / 2);
+        E[i + last + 2] = cc::addc(E[i + last + 2], 0);
       }
     }
-    w.l[15] = 0;
-    // double: shift the 512-bit off-diagonal sum left by one bit
-    w.l[15] = (w.l[15] << 1) | (w.l[14] >> 31);
+    // S = E + O (the off-diagonal sum, < 2^511), then 2S + diagonal
+    uint32_t S[16];
+    S[0] = cc::add_cc(E[0], O[0]);
 #pragma unroll
-    for (int k = 14; k > 0; k--)
-      w.l[k] = (w.l[k] << 1) | (w.l[k - 1] >> 31);
-    w.l[0] = w.l[0] << 1;
-    // add the diagonal a[i]^2 at words 2i, 2i+1
+    for (int k = 1; k < 15; k++)
+      S[k] = cc::addc_cc(E[k], O[k]);
+    S[15] = cc::addc(E[15], O[15]);
+    fe_wide w;
+    w.l[0] = cc::add_cc(S[0], S[0]);
+#pragma unroll
+    for (int k = 1; k < 15; k++)
+      w.l[k] = cc::addc_cc(S[k], S[k]);
+    w.l[15] = cc::addc(S[15], S[15]);
     w.l[0] = cc::mad_lo_cc(a.l[0], a.l[0], w.l[0]);
     w.l[1] = cc::madc_hi_cc(a.l[0], a.l[0], w.l[1]);
 #pragma unroll
-    for (int i = 1; i < 7; i++) {
-      w.l[2 * i] = cc::madc_lo_cc(a.l[i], a.l[i], w.l[2 * i]);
-      w.l[2 * i + 1] = cc::madc_hi_cc(a.l[i], a.l[i], w.l[2 * i + 1]);
+    for (int k = 1; k < 7; k++) {
+      w.l[2 * k] = cc::madc_lo_cc(a.l[k], a.l[k], w.l[2 * k]);
+      w.l[2 * k + 1] = cc::madc_hi_cc(a.l[k], a.l[k], w.l[2 * k + 1]);
     }
     w.l[14] = cc::madc_lo_cc(a.l[7], a.l[7], w.l[14]);
     w.l[15] = cc::madc_hi(a.l[7], a.l[7], w.l[15]);
@@ -542,30 +644,32 @@ template <class F> struct field {
   }
 
   // Montgomery reduction of a 512-bit value w < m*2^256:
-  // REDC(w) = REDC(w_lo) + w_hi, where REDC(w_lo) <= m; the result is < 2m
+  // REDC(w) = REDC(w_lo) + w_hi with REDC(w_lo) <= m; the result is < 2m
   // whenever w_hi < m (true for w < 4m^2).  136 multiply instructions.
   static BN_HD fe redc_wide(const fe_wide &w) {
-    uint32_t t0 = w.l[0], t1 = w.l[1], t2 = w.l[2], t3 = w.l[3], t4 = w.l[4], t5 = w.l[5], t6 = w.l[6], t7 = w.l[7], t8 = 0;
+    fe lo;
 #pragma unroll
-    for (int i = 0; i < 8; i++)
-      reduce_round(t0, t1, t2, t3, t4, t5, t6, t7, t8);
-    fe r;
-    r.l[0] = cc::add_cc(t0, w.l[8]);
-    r.l[1] = cc::addc_cc(t1, w.l[9]);
-    r.l[2] = cc::addc_cc(t2, w.l[10]);
-    r.l[3] = cc::addc_cc(t3, w.l[11]);
-    r.l[4] = cc::addc_cc(t4, w.l[12]);
-    r.l[5] = cc::addc_cc(t5, w.l[13]);
-    r.l[6] = cc::addc_cc(t6, w.l[14]);
-    r.l[7] = cc::addc(t7, w.l[15]);
-    return r;
+    for (int k = 0; k < 8; k++)
+      lo.l[k] = w.l[k];
+    const fe r = redc_low(lo);
+    fe out;
+    out.l[0] = cc::add_cc(r.l[0], w.l[8]);
+#pragma unroll
+    for (int k = 1; k < 7; k++)
+      out.l[k] = cc::addc_cc(r.l[k], w.l[k + 8]);
+    out.l[7] = cc::addc(r.l[7], w.l[15]);
+    return out;
   }
 
-  static BN_HD fe sqr(const fe &a) { return redc_wide(sqr_wide(a)); }
+#if defined(BN254_SQR_AS_MUL)
+  static BN_HD_MUL fe sqr(const fe &a) { return mul(a, a); }
+#else
+  static BN_HD_MUL fe sqr(const fe &a) { return redc_wide(sqr_wide(a)); }
+#endif
 
   // a*b - c*d with one reduction: both products < 4m^2; a negative
   // difference is lifted by 4m^2, so the reduced operand is in [0, 4m^2).
-  static BN_HD fe mul_sub_mul(const fe &a, const fe &b, const fe &c, const fe &d) {
+  static BN_HD_MUL fe mul_sub_mul(const fe &a, const fe &b, const fe &c, const fe &d) {
     fe_wide x = mul_wide(a, b);
     const fe_wide y = mul_wide(c, d);
     x.l[0] = cc::sub_cc(x.l[0], y.l[0]);
@@ -583,22 +687,7 @@ template <class F> struct field {
 
   // Montgomery -> standard form, fully reduced.  Any 256-bit input works:
   // REDC(a) <= m, and a result equal to m folds to 0.
-  static BN_HD fe from_mont(const fe &a) {
-    uint32_t t0 = a.l[0], t1 = a.l[1], t2 = a.l[2], t3 = a.l[3], t4 = a.l[4], t5 = a.l[5], t6 = a.l[6], t7 = a.l[7], t8 = 0;
-#pragma unroll
-    for (int i = 0; i < 8; i++)
-      reduce_round(t0, t1, t2, t3, t4, t5, t6, t7, t8);
-    fe r;
-    r.l[0] = t0;
-    r.l[1] = t1;
-    r.l[2] = t2;
-    r.l[3] = t3;
-    r.l[4] = t4;
-    r.l[5] = t5;
-    r.l[6] = t6;
-    r.l[7] = t7;
-    return reduce_full(r);
-  }
+  static BN_HD fe from_mont(const fe &a) { return reduce_full(redc_low(a)); }
 
   // standard -> Montgomery form (input < 2m), fully reduced
   static BN_HD fe to_mont(const fe &a) {

@@ -34,6 +34,30 @@ __global__ void __launch_bounds__(256) mad_peak_kernel(uint32_t seed, unsigned i
   sink[tid] = x;
 }
 
+// kinds 4 / 5: sixteen independent mad.lo (4) or mad.hi (5) per iteration
+template <bool HI> __global__ void __launch_bounds__(256) mad_half_kernel(uint32_t seed, unsigned iters, uint32_t *sink) {
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t acc[16];
+  const uint32_t b = seed ^ (tid * 0x9e3779b9u), c = seed + tid;
+#pragma unroll
+  for (int j = 0; j < 16; j++)
+    acc[j] = tid * (j + 3);
+  for (unsigned i = 0; i < iters; i++) {
+#pragma unroll
+    for (int j = 0; j < 16; j++) {
+      if (HI)
+        asm volatile("mad.hi.u32 %0, %0, %1, %2;" : "+r"(acc[j]) : "r"(b), "r"(c));
+      else
+        asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(acc[j]) : "r"(b), "r"(c));
+    }
+  }
+  uint32_t x = 0;
+#pragma unroll
+  for (int j = 0; j < 16; j++)
+    x ^= acc[j];
+  sink[tid] = x;
+}
+
 // kind 1: one 16-instruction carry chain per iteration (madc.lo.cc / madc.hi.cc)
 __global__ void __launch_bounds__(256) mad_chain_kernel(uint32_t seed, unsigned iters, uint32_t *sink) {
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -89,6 +113,47 @@ __global__ void __launch_bounds__(128) montmul_kernel(uint32_t seed, unsigned it
   sink[tid] = x.l[0] ^ z.l[1];
 }
 
+// kinds 6..9: component throughput (two independent chains per thread)
+//   6: squaring (208 multiply instructions), 7: a*b - c*d (392),
+//   8: 512-bit product (128), 9: field add + sub pairs (no multiplies; counted as 2 per pair)
+template <int KIND> __global__ void __launch_bounds__(128) component_kernel(uint32_t seed, unsigned iters, uint32_t *sink) {
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+  fe x, y, z, w;
+#pragma unroll
+  for (int j = 0; j < 8; j++) {
+    x.l[j] = (seed * (j + 7)) ^ tid;
+    y.l[j] = (seed + j) * 0x2545f491u;
+    z.l[j] = tid * (j + 1);
+    w.l[j] = (tid + j) * 0x9e3779b9u;
+  }
+  x.l[7] &= 0x1fffffff;
+  y.l[7] &= 0x1fffffff;
+  z.l[7] &= 0x1fffffff;
+  w.l[7] &= 0x1fffffff;
+  uint32_t acc = 0;
+  for (unsigned i = 0; i < iters; i++) {
+    if (KIND == 6) {
+      x = fq::sqr(x);
+      z = fq::sqr(z);
+    } else if (KIND == 7) {
+      x = fq::mul_sub_mul(x, y, z, w);
+      z = fq::mul_sub_mul(z, w, x, y);
+    } else if (KIND == 8) {
+      const fe_wide a = fq::mul_wide(x, y);
+      const fe_wide b = fq::mul_wide(z, w);
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        x.l[j] ^= a.l[j + 8];
+        z.l[j] ^= b.l[j] & 0x0fffffff;
+      }
+    } else {
+      x = fq::sub(fq::add(x, y), w);
+      z = fq::sub(fq::add(z, w), y);
+    }
+  }
+  sink[tid] = x.l[0] ^ z.l[1] ^ acc;
+}
+
 // kind 3: XYZZ += affine chain (never the doubling branch: acc = k*G, k >= 2)
 __global__ void __launch_bounds__(128) madd_kernel(unsigned iters, uint32_t *sink) {
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -109,7 +174,7 @@ __global__ void __launch_bounds__(128) madd_kernel(unsigned iters, uint32_t *sin
 } // namespace
 
 extern "C" bc_error msm_b200_measure_mul_throughput(unsigned kind, double *mulops_per_second) {
-  if (!mulops_per_second || kind > 3)
+  if (!mulops_per_second || kind > 9)
     return bc_error_invalid_value;
   int device = 0, sms = 0;
   cudaError_t e = cudaGetDevice(&device);
@@ -117,10 +182,17 @@ extern "C" bc_error msm_b200_measure_mul_throughput(unsigned kind, double *mulop
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   if (e != cudaSuccess)
     return static_cast<bc_error>(e);
-  const unsigned threads = kind < 2 ? 256 : 128;
-  const unsigned blocks = kind < 2 ? sms * 8 : sms * 4;
-  const unsigned iters = kind == 0 ? 65536 : kind == 1 ? 65536 : kind == 2 ? 4096 : 1024;
-  const double per_iter = kind == 0 ? 16.0 : kind == 1 ? 16.0 : kind == 2 ? 2.0 * 264 : 2392.0;
+  const bool light = kind < 2 || kind == 4 || kind == 5;
+  const unsigned threads = light ? 256 : 128;
+  const unsigned blocks = light ? sms * 8 : sms * 4;
+  const unsigned iters = light ? 65536 : kind == 2 ? 4096 : kind == 3 ? 1024 : kind == 9 ? 65536 : 4096;
+  const double per_iter = light ? 16.0
+                          : kind == 2 ? 2.0 * 264
+                          : kind == 3 ? 2392.0
+                          : kind == 6 ? 2.0 * 208
+                          : kind == 7 ? 2.0 * 392
+                          : kind == 8 ? 2.0 * 256
+                                      : 4.0;
   uint32_t *sink = nullptr;
   cudaStream_t stream = nullptr;
   cudaEvent_t start = nullptr, stop = nullptr;
@@ -139,6 +211,12 @@ extern "C" bc_error msm_b200_measure_mul_throughput(unsigned kind, double *mulop
       case 0: mad_peak_kernel<<<blocks, threads, 0, stream>>>(0x1234567u, iters, sink); break;
       case 1: mad_chain_kernel<<<blocks, threads, 0, stream>>>(0x1234567u, iters, sink); break;
       case 2: montmul_kernel<<<blocks, threads, 0, stream>>>(0x1234567u, iters, sink); break;
+      case 4: mad_half_kernel<false><<<blocks, threads, 0, stream>>>(0x1234567u, iters, sink); break;
+      case 5: mad_half_kernel<true><<<blocks, threads, 0, stream>>>(0x1234567u, iters, sink); break;
+      case 6: component_kernel<6><<<blocks, threads, 0, stream>>>(0x1234567u, iters, sink); break;
+      case 7: component_kernel<7><<<blocks, threads, 0, stream>>>(0x1234567u, iters, sink); break;
+      case 8: component_kernel<8><<<blocks, threads, 0, stream>>>(0x1234567u, iters, sink); break;
+      case 9: component_kernel<9><<<blocks, threads, 0, stream>>>(0x1234567u, iters, sink); break;
       default: madd_kernel<<<blocks, threads, 0, stream>>>(iters, sink); break;
       }
       if ((e = cudaGetLastError()) != cudaSuccess)

@@ -78,7 +78,8 @@ plan make_plan(unsigned n, unsigned window_bits, int sms) {
   const unsigned long long full = (unsigned long long)sms * 4 * ACC_THREADS;
   p.acc_threads = (unsigned)std::max(1ull, std::min(full, (entries + 7) / 8));
   p.merge_chunk = 4;
-  p.log_m = std::min(4u, p.log_b);
+  // groups of m = 8 slots: enough reduction threads to fill the GPU at c = 16
+  p.log_m = std::min(3u, p.log_b);
   p.log_g = p.log_b - p.log_m;
   p.groups = 1u << p.log_g;
   p.sum_fanin = 8;
@@ -87,7 +88,7 @@ plan make_plan(unsigned n, unsigned window_bits, int sms) {
 
 // Scratch layout inside one pool allocation.
 struct layout {
-  size_t keys[2], vals[2], counts, zeros, buckets, flags, hb[2], hp[2], tree[2], streams[2], results, scalars, bases, total;
+  size_t keys[2], vals[2], counts, digit_base, zeros, buckets, flags, hb[2], hp[2], tree[2], streams[2], results, scalars, bases, total;
 };
 
 static size_t align_up(size_t v) { return (v + 255) & ~(size_t)255; }
@@ -106,6 +107,7 @@ static layout make_layout(const plan &p, bool copy_scalars, bool copy_bases, boo
     l.vals[i] = take(entries * 4);
   }
   l.counts = take((size_t)p.windows * SORT_RADIX * p.tiles * 4);
+  l.digit_base = take((size_t)p.windows * SORT_RADIX * 4);
   l.zeros = take((size_t)p.windows * 4);
   const size_t slots = (size_t)p.windows << p.log_b;
   l.buckets = take(slots * sizeof(xyzz));
@@ -152,6 +154,7 @@ cudaError_t enqueue_pipeline(const plan &p, const fe *scalars, const affine *bas
   uint32_t *keys[2] = {reinterpret_cast<uint32_t *>(scratch + l.keys[0]), reinterpret_cast<uint32_t *>(scratch + l.keys[1])};
   uint32_t *vals[2] = {reinterpret_cast<uint32_t *>(scratch + l.vals[0]), reinterpret_cast<uint32_t *>(scratch + l.vals[1])};
   uint32_t *counts = reinterpret_cast<uint32_t *>(scratch + l.counts);
+  uint32_t *digit_base = reinterpret_cast<uint32_t *>(scratch + l.digit_base);
   uint32_t *zeros = reinterpret_cast<uint32_t *>(scratch + l.zeros);
   xyzz *buckets = reinterpret_cast<xyzz *>(scratch + l.buckets);
   uint8_t *flags = scratch + l.flags;
@@ -174,9 +177,14 @@ cudaError_t enqueue_pipeline(const plan &p, const fe *scalars, const affine *bas
     const dim3 grid(p.tiles, p.windows);
     sort_histogram_kernel<<<grid, SORT_THREADS, 0, stream>>>(keys[cur], n, p.tiles, shift, counts);
     CHECK(cudaGetLastError());
-    sort_scan_kernel<<<p.windows, 1024, 0, stream>>>(counts, p.tiles);
+    sort_scan_kernel<<<p.windows, 1024, 0, stream>>>(counts, p.tiles, digit_base);
     CHECK(cudaGetLastError());
-    sort_scatter_kernel<<<grid, SORT_THREADS, 0, stream>>>(keys[cur], vals[cur], keys[cur ^ 1], vals[cur ^ 1], n, p.tiles, shift, counts);
+    if (pass == 0)
+      sort_scatter_first_kernel<<<grid, SORT_THREADS, 0, stream>>>(keys[cur], vals[cur], keys[cur ^ 1], vals[cur ^ 1], n, p.tiles, shift, counts,
+                                                                    digit_base);
+    else
+      sort_scatter_stable_kernel<<<grid, SORT_THREADS, 0, stream>>>(keys[cur], vals[cur], keys[cur ^ 1], vals[cur ^ 1], n, p.tiles, shift, counts,
+                                                                   digit_base);
     CHECK(cudaGetLastError());
     launched += 3;
     cur ^= 1;

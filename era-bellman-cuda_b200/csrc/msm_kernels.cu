@@ -110,143 +110,230 @@ __global__ void __launch_bounds__(256) digits_kernel(const fe *__restrict__ scal
 
 // ---------------------------------------------------------------------------
 // 2. LSD radix sort, one 8-bit digit per pass, independent per window segment.
-//    counts / offsets layout per window: [digit][tile], so one exclusive scan
-//    of a window's array yields every (digit, tile) output offset.
+//    counts layout: [window][digit][tile]; after sort_scan_kernel it holds,
+//    per (window, digit), the exclusive prefix over tiles, and digit_base
+//    [window][digit] the exclusive prefix over digits: an element's output
+//    position is digit_base + counts + its rank among equal digits in the tile.
 // ---------------------------------------------------------------------------
+constexpr unsigned SORT_WARPS = SORT_THREADS / 32;
+
+__device__ __forceinline__ unsigned sort_digit(uint32_t key, unsigned shift) { return (key >> shift) & (SORT_RADIX - 1); }
+
+// Tile histogram: per-warp shared counters (no cross-warp contention); the
+// dominant zero digit of sparse scalars is counted with one ballot per warp.
 __global__ void __launch_bounds__(SORT_THREADS) sort_histogram_kernel(const uint32_t *__restrict__ keys, unsigned n, unsigned tiles,
                                                                       unsigned shift, uint32_t *__restrict__ counts) {
-  __shared__ uint32_t hist[SORT_RADIX];
-  const unsigned tile = blockIdx.x, w = blockIdx.y;
-  for (unsigned d = threadIdx.x; d < SORT_RADIX; d += blockDim.x)
-    hist[d] = 0;
-  __syncthreads();
-  const uint32_t *seg = keys + (size_t)w * n;
-  const unsigned lane = threadIdx.x & 31;
-#pragma unroll 4
-  for (unsigned k = 0; k < SORT_ITEMS; k++) {
-    const unsigned idx = tile * SORT_TILE + k * SORT_THREADS + threadIdx.x;
-    const unsigned d = idx < n ? (seg[idx] >> shift) & (SORT_RADIX - 1) : SORT_RADIX;
-    // warp-aggregated increment: one shared atomic per distinct digit
-    const unsigned peers = __match_any_sync(0xffffffffu, d);
-    if (d < SORT_RADIX && lane == (unsigned)(__ffs(peers) - 1))
-      atomicAdd(&hist[d], (unsigned)__popc(peers));
-  }
-  __syncthreads();
-  for (unsigned d = threadIdx.x; d < SORT_RADIX; d += blockDim.x)
-    counts[((size_t)w * SORT_RADIX + d) * tiles + tile] = hist[d];
-}
-
-// Exclusive scan of one window's [digit][tile] counts; one block per window.
-__global__ void __launch_bounds__(1024) sort_scan_kernel(uint32_t *counts, unsigned tiles) {
-  __shared__ uint32_t warp_sums[32];
-  __shared__ uint32_t carry_in;
-  const unsigned total = SORT_RADIX * tiles;
-  uint32_t *seg = counts + (size_t)blockIdx.x * total;
-  if (threadIdx.x == 0)
-    carry_in = 0;
-  __syncthreads();
-  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (unsigned base = 0; base < total; base += 4 * blockDim.x) {
-    uint32_t v[4];
-    uint32_t local = 0;
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-      const unsigned idx = base + 4 * threadIdx.x + k;
-      v[k] = idx < total ? seg[idx] : 0;
-      local += v[k];
-    }
-    // inclusive warp scan of the per-thread sums
-    uint32_t incl = local;
-#pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
-      const uint32_t t = __shfl_up_sync(0xffffffffu, incl, off);
-      if (lane >= (unsigned)off)
-        incl += t;
-    }
-    if (lane == 31)
-      warp_sums[warp] = incl;
-    __syncthreads();
-    if (warp == 0) {
-      uint32_t ws = lane < (blockDim.x >> 5) ? warp_sums[lane] : 0;
-#pragma unroll
-      for (int off = 1; off < 32; off <<= 1) {
-        const uint32_t t = __shfl_up_sync(0xffffffffu, ws, off);
-        if (lane >= (unsigned)off)
-          ws += t;
-      }
-      warp_sums[lane] = ws; // inclusive
-    }
-    __syncthreads();
-    uint32_t run = carry_in + (incl - local) + (warp > 0 ? warp_sums[warp - 1] : 0);
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-      const unsigned idx = base + 4 * threadIdx.x + k;
-      if (idx < total)
-        seg[idx] = run;
-      run += v[k];
-    }
-    __syncthreads();
-    if (threadIdx.x == blockDim.x - 1)
-      carry_in = run;
-    __syncthreads();
-  }
-}
-
-// Stable scatter.  Warp k of the block ranks the items of its sub-tile round by
-// round (32 consecutive items per round) with __match_any_sync; per-warp digit
-// counters then get an exclusive scan across warps and the tile's global
-// offset, which keeps the pass stable.
-__global__ void __launch_bounds__(SORT_THREADS) sort_scatter_kernel(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
-                                                                    uint32_t *__restrict__ keys_out, uint32_t *__restrict__ vals_out,
-                                                                    unsigned n, unsigned tiles, unsigned shift,
-                                                                    const uint32_t *__restrict__ offsets) {
-  constexpr unsigned WARPS = SORT_THREADS / 32;
-  __shared__ uint32_t whist[WARPS][SORT_RADIX];
+  __shared__ uint32_t hist[SORT_WARPS][SORT_RADIX];
   const unsigned tile = blockIdx.x, w = blockIdx.y;
   const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (unsigned d = lane; d < SORT_RADIX; d += 32)
-    whist[warp][d] = 0;
+    hist[warp][d] = 0;
   __syncwarp();
-  const size_t seg = (size_t)w * n;
-  const unsigned sub_base = tile * SORT_TILE + warp * (32 * SORT_ITEMS);
-  const unsigned lt_mask = (1u << lane) - 1;
-  uint32_t key[SORT_ITEMS], val[SORT_ITEMS], rank[SORT_ITEMS];
-#pragma unroll
-  for (unsigned r = 0; r < SORT_ITEMS; r++) {
-    const unsigned idx = sub_base + r * 32 + lane;
+  const uint32_t *seg = keys + (size_t)w * n;
+  const unsigned base = tile * SORT_TILE;
+#pragma unroll 4
+  for (unsigned k = 0; k < SORT_ITEMS; k++) {
+    const unsigned idx = base + k * SORT_THREADS + threadIdx.x;
     const bool valid = idx < n;
-    key[r] = valid ? keys_in[seg + idx] : 0;
-    val[r] = valid ? vals_in[seg + idx] : 0;
-    const unsigned d = valid ? (key[r] >> shift) & (SORT_RADIX - 1) : SORT_RADIX;
-    const unsigned peers = __match_any_sync(0xffffffffu, d);
-    const uint32_t before = valid ? whist[warp][d] : 0;
-    __syncwarp();
-    if (valid && lane == (unsigned)(__ffs(peers) - 1))
-      whist[warp][d] = before + __popc(peers);
-    __syncwarp();
-    rank[r] = before + __popc(peers & lt_mask);
+    const unsigned d = valid ? sort_digit(seg[idx], shift) : 0;
+    const unsigned zeros = __ballot_sync(0xffffffffu, valid && d == 0);
+    if (valid && d != 0)
+      atomicAdd(&hist[warp][d], 1u);
+    if (lane == 0 && zeros)
+      hist[warp][0] += __popc(zeros);
   }
   __syncthreads();
   for (unsigned d = threadIdx.x; d < SORT_RADIX; d += blockDim.x) {
-    uint32_t run = offsets[((size_t)w * SORT_RADIX + d) * tiles + tile];
+    uint32_t sum = 0;
 #pragma unroll
-    for (unsigned k = 0; k < WARPS; k++) {
-      const uint32_t t = whist[k][d];
-      whist[k][d] = run;
-      run += t;
+    for (unsigned k = 0; k < SORT_WARPS; k++)
+      sum += hist[k][d];
+    counts[((size_t)w * SORT_RADIX + d) * tiles + tile] = sum;
+  }
+}
+
+// One block per window, one warp per digit row: exclusive prefix over tiles
+// in place, then the exclusive prefix of the digit totals into digit_base.
+__global__ void __launch_bounds__(1024) sort_scan_kernel(uint32_t *counts, unsigned tiles, uint32_t *__restrict__ digit_base) {
+  __shared__ uint32_t totals[SORT_RADIX];
+  const unsigned w = blockIdx.x;
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+  for (unsigned d = warp; d < SORT_RADIX; d += warps) {
+    uint32_t *row = counts + ((size_t)w * SORT_RADIX + d) * tiles;
+    uint32_t carry = 0;
+    for (unsigned t0 = 0; t0 < tiles; t0 += 32) {
+      const unsigned t = t0 + lane;
+      const uint32_t v = t < tiles ? row[t] : 0;
+      uint32_t incl = v;
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t u = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= (unsigned)off)
+          incl += u;
+      }
+      if (t < tiles)
+        row[t] = carry + incl - v;
+      carry += __shfl_sync(0xffffffffu, incl, 31);
+    }
+    if (lane == 0)
+      totals[d] = carry;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    // 256 totals, 8 per lane
+    uint32_t v[SORT_RADIX / 32], local = 0;
+#pragma unroll
+    for (unsigned k = 0; k < SORT_RADIX / 32; k++) {
+      v[k] = totals[lane * (SORT_RADIX / 32) + k];
+      local += v[k];
+    }
+    uint32_t incl = local;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const uint32_t u = __shfl_up_sync(0xffffffffu, incl, off);
+      if (lane >= (unsigned)off)
+        incl += u;
+    }
+    uint32_t run = incl - local;
+#pragma unroll
+    for (unsigned k = 0; k < SORT_RADIX / 32; k++) {
+      digit_base[(size_t)w * SORT_RADIX + lane * (SORT_RADIX / 32) + k] = run;
+      run += v[k];
+    }
+  }
+}
+
+// Exclusive block-wide scan of 256 shared counters by the first 256 threads.
+__device__ __forceinline__ void scan_256(const uint32_t *in, uint32_t *out, uint32_t *warp_sums) {
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t v = 0, incl = 0;
+  if (threadIdx.x < SORT_RADIX) {
+    v = in[threadIdx.x];
+    incl = v;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const uint32_t u = __shfl_up_sync(0xffffffffu, incl, off);
+      if (lane >= (unsigned)off)
+        incl += u;
+    }
+    if (lane == 31)
+      warp_sums[warp] = incl;
+  }
+  __syncthreads();
+  if (threadIdx.x < SORT_RADIX) {
+    uint32_t before = 0;
+    for (unsigned k = 0; k < warp; k++)
+      before += warp_sums[k];
+    out[threadIdx.x] = before + incl - v;
+  }
+  __syncthreads();
+}
+
+// Scatter one tile.  Ranks among equal digits: STABLE (every pass after the
+// first, which LSD order requires) ranks warp by warp, 32 consecutive items
+// per round with __match_any_sync; the first pass may take any order and
+// ranks with shared atomics.  The tile is then reordered in shared memory so
+// that each digit's run is written to global memory with consecutive
+// addresses.
+template <bool STABLE>
+__device__ __forceinline__ void sort_scatter_tile(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
+                                                  uint32_t *__restrict__ keys_out, uint32_t *__restrict__ vals_out, unsigned n, unsigned tiles,
+                                                  unsigned shift, const uint32_t *__restrict__ counts, const uint32_t *__restrict__ digit_base) {
+  __shared__ uint32_t s_key[SORT_TILE];
+  __shared__ uint32_t s_val[SORT_TILE];
+  __shared__ uint32_t whist[STABLE ? SORT_WARPS : 1][SORT_RADIX];
+  __shared__ uint32_t tile_cnt[SORT_RADIX], tile_off[SORT_RADIX], glob[SORT_RADIX], warp_sums[SORT_WARPS];
+  const unsigned tile = blockIdx.x, w = blockIdx.y;
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const size_t seg = (size_t)w * n;
+  const unsigned base = tile * SORT_TILE;
+  const unsigned count = min(SORT_TILE, n - base);
+  const unsigned sub = warp * (32 * SORT_ITEMS); // this warp's items: base + sub + r*32 + lane
+  if (STABLE) {
+    for (unsigned d = lane; d < SORT_RADIX; d += 32)
+      whist[warp][d] = 0;
+  } else {
+    for (unsigned d = threadIdx.x; d < SORT_RADIX; d += blockDim.x)
+      tile_cnt[d] = 0;
+  }
+  __syncthreads();
+  uint32_t key[SORT_ITEMS], val[SORT_ITEMS], rank[SORT_ITEMS];
+  const unsigned lt_mask = (1u << lane) - 1;
+#pragma unroll
+  for (unsigned r = 0; r < SORT_ITEMS; r++) {
+    const unsigned i = sub + r * 32 + lane;
+    const bool valid = i < count;
+    key[r] = valid ? keys_in[seg + base + i] : 0;
+    val[r] = valid ? vals_in[seg + base + i] : 0;
+    const unsigned d = valid ? sort_digit(key[r], shift) : SORT_RADIX;
+    if (STABLE) {
+      const unsigned peers = __match_any_sync(0xffffffffu, d);
+      const uint32_t before = valid ? whist[warp][d] : 0;
+      __syncwarp();
+      if (valid && lane == (unsigned)(__ffs(peers) - 1))
+        whist[warp][d] = before + __popc(peers);
+      __syncwarp();
+      rank[r] = before + __popc(peers & lt_mask);
+    } else {
+      rank[r] = valid ? atomicAdd(&tile_cnt[d], 1u) : 0;
     }
   }
   __syncthreads();
+  if (STABLE) {
+    // per digit: exclusive prefix over warps (warp order = item order)
+    for (unsigned d = threadIdx.x; d < SORT_RADIX; d += blockDim.x) {
+      uint32_t run = 0;
+#pragma unroll
+      for (unsigned k = 0; k < SORT_WARPS; k++) {
+        const uint32_t t = whist[k][d];
+        whist[k][d] = run;
+        run += t;
+      }
+      tile_cnt[d] = run;
+    }
+    __syncthreads();
+  }
+  scan_256(tile_cnt, tile_off, warp_sums);
+  for (unsigned d = threadIdx.x; d < SORT_RADIX; d += blockDim.x)
+    glob[d] = digit_base[(size_t)w * SORT_RADIX + d] + counts[((size_t)w * SORT_RADIX + d) * tiles + tile];
 #pragma unroll
   for (unsigned r = 0; r < SORT_ITEMS; r++) {
-    const unsigned idx = sub_base + r * 32 + lane;
-    if (idx < n) {
-      const unsigned d = (key[r] >> shift) & (SORT_RADIX - 1);
-      const uint32_t pos = whist[warp][d] + rank[r];
-      keys_out[seg + pos] = key[r];
-      vals_out[seg + pos] = val[r];
+    const unsigned i = sub + r * 32 + lane;
+    if (i < count) {
+      const unsigned d = sort_digit(key[r], shift);
+      const unsigned pos = tile_off[d] + (STABLE ? whist[warp][d] : 0) + rank[r];
+      s_key[pos] = key[r];
+      s_val[pos] = val[r];
     }
   }
+  __syncthreads();
+#pragma unroll 4
+  for (unsigned j = 0; j < SORT_ITEMS; j++) {
+    const unsigned pos = j * SORT_THREADS + threadIdx.x;
+    if (pos < count) {
+      const uint32_t k = s_key[pos];
+      const unsigned d = sort_digit(k, shift);
+      const size_t out = seg + glob[d] + (pos - tile_off[d]);
+      keys_out[out] = k;
+      vals_out[out] = s_val[pos];
+    }
+  }
+}
+
+__global__ void __launch_bounds__(SORT_THREADS) sort_scatter_first_kernel(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
+                                                                          uint32_t *__restrict__ keys_out, uint32_t *__restrict__ vals_out,
+                                                                          unsigned n, unsigned tiles, unsigned shift,
+                                                                          const uint32_t *__restrict__ counts,
+                                                                          const uint32_t *__restrict__ digit_base) {
+  sort_scatter_tile<false>(keys_in, vals_in, keys_out, vals_out, n, tiles, shift, counts, digit_base);
+}
+
+__global__ void __launch_bounds__(SORT_THREADS) sort_scatter_stable_kernel(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
+                                                                           uint32_t *__restrict__ keys_out, uint32_t *__restrict__ vals_out,
+                                                                           unsigned n, unsigned tiles, unsigned shift,
+                                                                           const uint32_t *__restrict__ counts,
+                                                                           const uint32_t *__restrict__ digit_base) {
+  sort_scatter_tile<true>(keys_in, vals_in, keys_out, vals_out, n, tiles, shift, counts, digit_base);
 }
 
 // ---------------------------------------------------------------------------
@@ -272,6 +359,9 @@ __global__ void zero_counts_kernel(const uint32_t *__restrict__ keys, unsigned n
 // 4. accumulation
 // ---------------------------------------------------------------------------
 constexpr unsigned MAX_WINDOWS = 128;
+#ifndef ACC_MIN_BLOCKS
+#define ACC_MIN_BLOCKS 4 // resident accumulation blocks per SM (caps registers at 128)
+#endif
 
 struct entry_cursor {
   size_t idx;       // physical index into keys / vals
@@ -291,14 +381,19 @@ __device__ __forceinline__ void cursor_advance(entry_cursor &cur, unsigned n, un
   }
 }
 
+// A base's y is never 0 (BN254 G1 has odd order, so no point has y = 0):
+// its negation is 2p - y.
 __device__ __forceinline__ affine signed_base(const affine *__restrict__ bases, uint32_t val) {
   affine p = load_affine(bases + (val & 0x7fffffffu));
-  if (val >> 31)
-    p.y = fq::neg(p.y);
+  const fe ny = fq::neg_nonzero(p.y);
+  const bool negative = val >> 31;
+#pragma unroll
+  for (int i = 0; i < 8; i++)
+    p.y.l[i] = negative ? ny.l[i] : p.y.l[i];
   return p;
 }
 
-__global__ void __launch_bounds__(ACC_THREADS) accumulate_kernel(const uint32_t *__restrict__ keys, const uint32_t *__restrict__ vals,
+__global__ void __launch_bounds__(ACC_THREADS, ACC_MIN_BLOCKS) accumulate_kernel(const uint32_t *__restrict__ keys, const uint32_t *__restrict__ vals,
                                                                  const affine *__restrict__ bases, unsigned n, unsigned windows, unsigned log_b,
                                                                  const uint32_t *__restrict__ zeros, unsigned total_threads,
                                                                  xyzz *__restrict__ buckets, uint8_t *__restrict__ flags,
@@ -346,6 +441,7 @@ __global__ void __launch_bounds__(ACC_THREADS) accumulate_kernel(const uint32_t 
   const bool continued = cur.idx > (size_t)w * n + s_zeros[w] && keys[cur.idx - 1] == key;
   unsigned bucket = (cur.w << log_b) | (key & slot_mask);
   xyzz acc = curve::from_affine(signed_base(bases, val));
+  bool acc_inf = false; // a partial sum can cancel to infinity (p + (-p))
   bool first = true;
   const unsigned long long count = end - beg;
   for (unsigned long long k = 1; k < count; k++) {
@@ -355,6 +451,8 @@ __global__ void __launch_bounds__(ACC_THREADS) accumulate_kernel(const uint32_t 
     const unsigned b = (cur.w << log_b) | (key & slot_mask);
     const affine p = signed_base(bases, val);
     if (b != bucket) {
+      if (acc_inf)
+        acc = curve::infinity();
       if (first && continued) {
         head_bucket[t] = bucket;
         store_xyzz(head_point + t, acc);
@@ -365,10 +463,16 @@ __global__ void __launch_bounds__(ACC_THREADS) accumulate_kernel(const uint32_t 
       first = false;
       bucket = b;
       acc = curve::from_affine(p);
+      acc_inf = false;
+    } else if (acc_inf) {
+      acc = curve::from_affine(p);
+      acc_inf = false;
     } else {
-      acc = curve::add_affine(acc, p);
+      acc = curve::add_affine_finite(acc, p, acc_inf);
     }
   }
+  if (acc_inf)
+    acc = curve::infinity();
   if (first && continued) {
     head_bucket[t] = bucket;
     store_xyzz(head_point + t, acc);

@@ -76,10 +76,14 @@ __global__ void digits_kernel(const fe *__restrict__ scalars, unsigned n, unsign
 // ---------------------------------------------------------------------------
 __global__ void sort_histogram_kernel(const uint32_t *__restrict__ keys, unsigned n, unsigned tiles, unsigned shift,
                                       uint32_t *__restrict__ counts);
-__global__ void sort_scan_kernel(uint32_t *counts, unsigned tiles);
-__global__ void sort_scatter_kernel(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in, uint32_t *__restrict__ keys_out,
-                                    uint32_t *__restrict__ vals_out, unsigned n, unsigned tiles, unsigned shift,
-                                    const uint32_t *__restrict__ offsets);
+__global__ void sort_scan_kernel(uint32_t *counts, unsigned tiles, uint32_t *__restrict__ digit_base);
+// first pass (any order among equal digits) and later passes (stable)
+__global__ void sort_scatter_first_kernel(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in, uint32_t *__restrict__ keys_out,
+                                          uint32_t *__restrict__ vals_out, unsigned n, unsigned tiles, unsigned shift,
+                                          const uint32_t *__restrict__ counts, const uint32_t *__restrict__ digit_base);
+__global__ void sort_scatter_stable_kernel(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in, uint32_t *__restrict__ keys_out,
+                                           uint32_t *__restrict__ vals_out, unsigned n, unsigned tiles, unsigned shift,
+                                           const uint32_t *__restrict__ counts, const uint32_t *__restrict__ digit_base);
 
 // ---------------------------------------------------------------------------
 // 3. zero counts

@@ -55,6 +55,9 @@ bc_error msm_b200_execute_staged_async(const msm_b200_configuration *configurati
  *   kind 1: carry chains of madc.lo.cc / madc.hi.cc pairs
  *   kind 2: Fq Montgomery products (264 multiply instructions each)
  *   kind 3: XYZZ + affine mixed additions (2392 multiply instructions each)
+ *   kind 4: independent mad.lo only;  kind 5: independent mad.hi only
+ *   kinds 6..9: squaring, a*b - c*d, 512-bit products, add/sub pairs (the
+ *   last reports field additions per second, not multiply instructions)
  * Synchronous; about 0.1 s. */
 bc_error msm_b200_measure_mul_throughput(unsigned kind, double *mulops_per_second);
 

@@ -32,6 +32,7 @@ void fc_fq_op(int op, const uint32_t *a, const uint32_t *b, uint32_t *out, int n
     case 7: r = fq::to_mont(x); break;
     case 8: r = fq::inverse(x); break;
     case 9: r = fq::dbl(x); break;
+    case 10: r = fq::neg_nonzero(x); break;
     }
     st(out + 8 * i, r);
   }
@@ -61,6 +62,11 @@ int fc_fq_is_zero(const uint32_t *a) { return fq::is_zero(ld<fe>(a)) ? 1 : 0; }
 
 // curve: xyzz (32 words), affine (16 words), jacobian (24 words)
 void fc_add_affine(const uint32_t *p, const uint32_t *a, uint32_t *out) { st(out, curve::add_affine(ld<xyzz>(p), ld<affine>(a))); }
+int fc_add_affine_finite(const uint32_t *p, const uint32_t *a, uint32_t *out) {
+  bool inf = false;
+  st(out, curve::add_affine_finite(ld<xyzz>(p), ld<affine>(a), inf));
+  return inf ? 1 : 0;
+}
 void fc_add(const uint32_t *p, const uint32_t *q, uint32_t *out) { st(out, curve::add(ld<xyzz>(p), ld<xyzz>(q))); }
 void fc_dbl(const uint32_t *p, uint32_t *out) { st(out, curve::dbl(ld<xyzz>(p))); }
 void fc_from_affine(const uint32_t *a, uint32_t *out) { st(out, curve::from_affine(ld<affine>(a))); }

@@ -50,6 +50,15 @@ OPS = {
 }
 
 
+def test_neg_nonzero(field_check, pairs):
+    xs = [x for x in pairs[0] if 0 < x < 2 * P]
+    a = arr(xs)
+    out = np.zeros_like(a)
+    field_check.fc_fq_op(10, ptr(a), ptr(a), ptr(out), len(xs))
+    for x, r in zip(xs, ints(out)):
+        assert 0 < r < 2 * P and (r + x) % P == 0
+
+
 @pytest.mark.parametrize("op", sorted(OPS))
 def test_fq_ops(field_check, pairs, op):
     xs, ys = pairs
@@ -133,6 +142,11 @@ def test_curve_identities(field_check, oracle):
         neg = affine_mont((table[i][0], P - table[i][1]))
         f.fc_add_affine(ptr(p), ptr(neg), ptr(out))  # x - x
         assert xyzz_to_affine(out)[0]
+        assert f.fc_add_affine_finite(ptr(p), ptr(neg), ptr(out)) == 1  # flagged, not computed
+        assert f.fc_add_affine_finite(ptr(p), ptr(g), ptr(out)) == 0
+        assert xyzz_to_affine(out) == (False, *table[i + 1])
+        assert f.fc_add_affine_finite(ptr(p), ptr(a), ptr(out)) == 0  # doubling branch
+        assert xyzz_to_affine(out) == (False, *table[2 * i + 1])
         f.fc_dbl(ptr(p), ptr(out))
         assert xyzz_to_affine(out) == (False, *table[2 * i + 1])
         q = out.copy()
