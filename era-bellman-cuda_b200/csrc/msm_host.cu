@@ -88,7 +88,7 @@ plan make_plan(unsigned n, unsigned window_bits, int sms) {
 
 // Scratch layout inside one pool allocation.
 struct layout {
-  size_t keys[2], vals[2], counts, digit_base, zeros, buckets, flags, hb[2], hp[2], tree[2], streams[2], results, scalars, bases, total;
+  size_t keys[2], vals[2], counts, totals, zeros, buckets, flags, hb[2], hp[2], tree[2], streams[2], results, scalars, bases, total;
 };
 
 static size_t align_up(size_t v) { return (v + 255) & ~(size_t)255; }
@@ -107,7 +107,7 @@ static layout make_layout(const plan &p, bool copy_scalars, bool copy_bases, boo
     l.vals[i] = take(entries * 4);
   }
   l.counts = take((size_t)p.windows * SORT_RADIX * p.tiles * 4);
-  l.digit_base = take((size_t)p.windows * SORT_RADIX * 4);
+  l.totals = take((size_t)p.windows * SORT_RADIX * 4);
   l.zeros = take((size_t)p.windows * 4);
   const size_t slots = (size_t)p.windows << p.log_b;
   l.buckets = take(slots * sizeof(xyzz));
@@ -154,7 +154,7 @@ cudaError_t enqueue_pipeline(const plan &p, const fe *scalars, const affine *bas
   uint32_t *keys[2] = {reinterpret_cast<uint32_t *>(scratch + l.keys[0]), reinterpret_cast<uint32_t *>(scratch + l.keys[1])};
   uint32_t *vals[2] = {reinterpret_cast<uint32_t *>(scratch + l.vals[0]), reinterpret_cast<uint32_t *>(scratch + l.vals[1])};
   uint32_t *counts = reinterpret_cast<uint32_t *>(scratch + l.counts);
-  uint32_t *digit_base = reinterpret_cast<uint32_t *>(scratch + l.digit_base);
+  uint32_t *totals = reinterpret_cast<uint32_t *>(scratch + l.totals);
   uint32_t *zeros = reinterpret_cast<uint32_t *>(scratch + l.zeros);
   xyzz *buckets = reinterpret_cast<xyzz *>(scratch + l.buckets);
   uint8_t *flags = scratch + l.flags;
@@ -164,29 +164,39 @@ cudaError_t enqueue_pipeline(const plan &p, const fe *scalars, const affine *bas
   xyzz *streams[2] = {reinterpret_cast<xyzz *>(scratch + l.streams[0]), reinterpret_cast<xyzz *>(scratch + l.streams[1])};
   const unsigned n = p.n;
 
-  // 1. digits
-  digits_kernel<<<(n + 255) / 256, 256, 0, stream>>>(scalars, n, p.c, p.windows, keys[0], vals[0]);
+  // 1. digits (with the first sort pass's histograms when they fit in shared memory)
+  const bool fused_histogram = p.windows <= MAX_FUSED_HISTOGRAM_WINDOWS;
+  if (fused_histogram) {
+    digits_histogram_kernel<<<p.tiles, SORT_THREADS, p.windows * SORT_RADIX * 4, stream>>>(scalars, n, p.c, p.windows, p.tiles, keys[0],
+                                                                                            vals[0], counts);
+  } else {
+    digits_kernel<<<(n + 255) / 256, 256, 0, stream>>>(scalars, n, p.c, p.windows, keys[0], vals[0]);
+  }
   CHECK(cudaGetLastError());
   launched++;
   CHECK(mark());
 
   // 2. sort, 8 bits per pass
   int cur = 0;
+  const unsigned rows = p.windows * SORT_RADIX;
   for (unsigned pass = 0; pass < p.sort_passes; pass++) {
     const unsigned shift = pass * SORT_RADIX_BITS;
     const dim3 grid(p.tiles, p.windows);
-    sort_histogram_kernel<<<grid, SORT_THREADS, 0, stream>>>(keys[cur], n, p.tiles, shift, counts);
-    CHECK(cudaGetLastError());
-    sort_scan_kernel<<<p.windows, 1024, 0, stream>>>(counts, p.tiles, digit_base);
+    if (pass > 0 || !fused_histogram) {
+      sort_histogram_kernel<<<grid, SORT_THREADS, 0, stream>>>(keys[cur], n, p.tiles, shift, counts);
+      CHECK(cudaGetLastError());
+      launched++;
+    }
+    sort_scan_kernel<<<(rows * 32 + 255) / 256, 256, 0, stream>>>(counts, p.tiles, rows, totals);
     CHECK(cudaGetLastError());
     if (pass == 0)
       sort_scatter_first_kernel<<<grid, SORT_THREADS, 0, stream>>>(keys[cur], vals[cur], keys[cur ^ 1], vals[cur ^ 1], n, p.tiles, shift, counts,
-                                                                    digit_base);
+                                                                   totals);
     else
       sort_scatter_stable_kernel<<<grid, SORT_THREADS, 0, stream>>>(keys[cur], vals[cur], keys[cur ^ 1], vals[cur ^ 1], n, p.tiles, shift, counts,
-                                                                   digit_base);
+                                                                    totals);
     CHECK(cudaGetLastError());
-    launched += 3;
+    launched += 2;
     cur ^= 1;
   }
   CHECK(mark());
@@ -372,18 +382,25 @@ cudaError_t execute(const execution &e) {
   return status != cudaSuccess ? status : free_status;
 }
 
-template <class F> static cudaError_t set_l1_preference(F *func) {
-  CHECK(cudaFuncSetAttribute(func, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxL1));
+#ifndef ACC_CARVEOUT
+#define ACC_CARVEOUT 40
+#endif
+
+// Shared-memory carveout preference (percent of the maximum): as much L1 as
+// still lets the kernel reach its full occupancy.
+template <class F> static cudaError_t set_carveout(F *func, int percent) {
+  CHECK(cudaFuncSetAttribute(func, cudaFuncAttributePreferredSharedMemoryCarveout, percent));
   return cudaSuccess;
 }
 
 cudaError_t set_up() {
-  CHECK(set_l1_preference(accumulate_kernel));
-  CHECK(set_l1_preference(merge_heads_kernel));
-  CHECK(set_l1_preference(reduce_groups_kernel));
-  CHECK(set_l1_preference(reduce_tree_kernel));
-  CHECK(set_l1_preference(reduce_streams_kernel));
-  CHECK(set_l1_preference(digits_kernel));
+  CHECK(cudaFuncSetAttribute(digits_histogram_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             MAX_FUSED_HISTOGRAM_WINDOWS * SORT_RADIX * 4));
+  CHECK(set_carveout(accumulate_kernel, ACC_CARVEOUT)); // 4 blocks x 18 KB of base-point slots
+  CHECK(set_carveout(merge_heads_kernel, cudaSharedmemCarveoutMaxL1));
+  CHECK(set_carveout(reduce_groups_kernel, cudaSharedmemCarveoutMaxL1));
+  CHECK(set_carveout(reduce_tree_kernel, cudaSharedmemCarveoutMaxL1));
+  CHECK(set_carveout(reduce_streams_kernel, cudaSharedmemCarveoutMaxL1));
   return cudaSuccess;
 }
 

@@ -28,6 +28,9 @@ struct execution {
   unsigned *launches;              // optional: kernels enqueued
 };
 
+// windows whose first-pass histograms the digit kernel builds in shared memory
+constexpr unsigned MAX_FUSED_HISTOGRAM_WINDOWS = 48;
+
 // stages timed by msm_b200_execute_profiled
 constexpr unsigned PROFILE_STAGES = 6;
 

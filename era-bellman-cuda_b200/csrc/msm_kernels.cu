@@ -69,11 +69,8 @@ __device__ __forceinline__ uint32_t limb_at(const fe &s, unsigned k) {
 // ---------------------------------------------------------------------------
 // 1. digits
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) digits_kernel(const fe *__restrict__ scalars, unsigned n, unsigned c, unsigned windows,
-                                                     uint32_t *__restrict__ keys, uint32_t *__restrict__ vals) {
-  const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n)
-    return;
+// Signed windows of one scalar; emit(w, key, negative) for each window.
+template <class EMIT> __device__ __forceinline__ void scalar_digits(const fe *__restrict__ scalars, unsigned i, unsigned c, unsigned windows, EMIT emit) {
   fe s = fr::from_mont(load_fe_streaming(scalars + i)); // canonical, < r
   // r - s (s == 0 gives r, which is never the smaller one)
   const fe m = fr::modulus();
@@ -102,10 +99,47 @@ __global__ void __launch_bounds__(256) digits_kernel(const fe *__restrict__ scal
     } else {
       carry = 0;
     }
-    const size_t out = (size_t)w * n + i;
-    keys[out] = raw;
-    vals[out] = i | ((negative ^ (flip ? 1u : 0u)) << 31);
+    emit(w, raw, negative ^ (flip ? 1u : 0u));
   }
+}
+
+__global__ void __launch_bounds__(256) digits_kernel(const fe *__restrict__ scalars, unsigned n, unsigned c, unsigned windows,
+                                                     uint32_t *__restrict__ keys, uint32_t *__restrict__ vals) {
+  const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n)
+    return;
+  scalar_digits(scalars, i, c, windows, [&](unsigned w, uint32_t key, uint32_t negative) {
+    const size_t out = (size_t)w * n + i;
+    keys[out] = key;
+    vals[out] = i | (negative << 31);
+  });
+}
+
+// The same, one block per sort tile (SORT_TILE scalars), also producing the
+// first radix pass's tile histograms (low 8 bits of every window's keys), so
+// that pass needs no histogram kernel.  Dynamic shared memory: windows x 256
+// counters.
+__global__ void __launch_bounds__(SORT_THREADS) digits_histogram_kernel(const fe *__restrict__ scalars, unsigned n, unsigned c, unsigned windows,
+                                                                        unsigned tiles, uint32_t *__restrict__ keys, uint32_t *__restrict__ vals,
+                                                                        uint32_t *__restrict__ counts) {
+  extern __shared__ uint32_t hist[]; // [windows][SORT_RADIX]
+  const unsigned tile = blockIdx.x;
+  for (unsigned k = threadIdx.x; k < windows * SORT_RADIX; k += blockDim.x)
+    hist[k] = 0;
+  __syncthreads();
+  for (unsigned k = 0; k < SORT_ITEMS; k++) {
+    const unsigned i = tile * SORT_TILE + k * SORT_THREADS + threadIdx.x;
+    if (i < n)
+      scalar_digits(scalars, i, c, windows, [&](unsigned w, uint32_t key, uint32_t negative) {
+        const size_t out = (size_t)w * n + i;
+        keys[out] = key;
+        vals[out] = i | (negative << 31);
+        atomicAdd(&hist[w * SORT_RADIX + (key & (SORT_RADIX - 1))], 1u);
+      });
+  }
+  __syncthreads();
+  for (unsigned k = threadIdx.x; k < windows * SORT_RADIX; k += blockDim.x)
+    counts[(size_t)k * tiles + tile] = hist[k]; // k = w * 256 + d
 }
 
 // ---------------------------------------------------------------------------
@@ -152,55 +186,35 @@ __global__ void __launch_bounds__(SORT_THREADS) sort_histogram_kernel(const uint
   }
 }
 
-// One block per window, one warp per digit row: exclusive prefix over tiles
-// in place, then the exclusive prefix of the digit totals into digit_base.
-__global__ void __launch_bounds__(1024) sort_scan_kernel(uint32_t *counts, unsigned tiles, uint32_t *__restrict__ digit_base) {
-  __shared__ uint32_t totals[SORT_RADIX];
-  const unsigned w = blockIdx.x;
-  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
-  for (unsigned d = warp; d < SORT_RADIX; d += warps) {
-    uint32_t *row = counts + ((size_t)w * SORT_RADIX + d) * tiles;
-    uint32_t carry = 0;
-    for (unsigned t0 = 0; t0 < tiles; t0 += 32) {
-      const unsigned t = t0 + lane;
-      const uint32_t v = t < tiles ? row[t] : 0;
-      uint32_t incl = v;
+// One warp per (window, digit) row of counts: exclusive prefix over tiles in
+// place, the row total into totals[window][digit].  Lane l scans a contiguous
+// chunk of the row; the chunk sums are scanned across the warp.
+__global__ void __launch_bounds__(256) sort_scan_kernel(uint32_t *counts, unsigned tiles, unsigned rows, uint32_t *__restrict__ totals) {
+  const unsigned row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const unsigned lane = threadIdx.x & 31;
+  if (row >= rows)
+    return;
+  uint32_t *r = counts + (size_t)row * tiles;
+  const unsigned chunk = (tiles + 31) / 32;
+  const unsigned beg = min(tiles, lane * chunk), end = min(tiles, beg + chunk);
+  uint32_t local = 0;
+  for (unsigned t = beg; t < end; t++)
+    local += r[t];
+  uint32_t incl = local;
 #pragma unroll
-      for (int off = 1; off < 32; off <<= 1) {
-        const uint32_t u = __shfl_up_sync(0xffffffffu, incl, off);
-        if (lane >= (unsigned)off)
-          incl += u;
-      }
-      if (t < tiles)
-        row[t] = carry + incl - v;
-      carry += __shfl_sync(0xffffffffu, incl, 31);
-    }
-    if (lane == 0)
-      totals[d] = carry;
+  for (int off = 1; off < 32; off <<= 1) {
+    const uint32_t u = __shfl_up_sync(0xffffffffu, incl, off);
+    if (lane >= (unsigned)off)
+      incl += u;
   }
-  __syncthreads();
-  if (warp == 0) {
-    // 256 totals, 8 per lane
-    uint32_t v[SORT_RADIX / 32], local = 0;
-#pragma unroll
-    for (unsigned k = 0; k < SORT_RADIX / 32; k++) {
-      v[k] = totals[lane * (SORT_RADIX / 32) + k];
-      local += v[k];
-    }
-    uint32_t incl = local;
-#pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
-      const uint32_t u = __shfl_up_sync(0xffffffffu, incl, off);
-      if (lane >= (unsigned)off)
-        incl += u;
-    }
-    uint32_t run = incl - local;
-#pragma unroll
-    for (unsigned k = 0; k < SORT_RADIX / 32; k++) {
-      digit_base[(size_t)w * SORT_RADIX + lane * (SORT_RADIX / 32) + k] = run;
-      run += v[k];
-    }
+  uint32_t run = incl - local;
+  for (unsigned t = beg; t < end; t++) {
+    const uint32_t v = r[t];
+    r[t] = run;
+    run += v;
   }
+  if (lane == 31)
+    totals[row] = incl;
 }
 
 // Exclusive block-wide scan of 256 shared counters by the first 256 threads.
@@ -238,11 +252,11 @@ __device__ __forceinline__ void scan_256(const uint32_t *in, uint32_t *out, uint
 template <bool STABLE>
 __device__ __forceinline__ void sort_scatter_tile(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
                                                   uint32_t *__restrict__ keys_out, uint32_t *__restrict__ vals_out, unsigned n, unsigned tiles,
-                                                  unsigned shift, const uint32_t *__restrict__ counts, const uint32_t *__restrict__ digit_base) {
+                                                  unsigned shift, const uint32_t *__restrict__ counts, const uint32_t *__restrict__ totals) {
   __shared__ uint32_t s_key[SORT_TILE];
   __shared__ uint32_t s_val[SORT_TILE];
   __shared__ uint32_t whist[STABLE ? SORT_WARPS : 1][SORT_RADIX];
-  __shared__ uint32_t tile_cnt[SORT_RADIX], tile_off[SORT_RADIX], glob[SORT_RADIX], warp_sums[SORT_WARPS];
+  __shared__ uint32_t tile_cnt[SORT_RADIX], tile_off[SORT_RADIX], glob[SORT_RADIX], digit_base[SORT_RADIX], warp_sums[SORT_WARPS];
   const unsigned tile = blockIdx.x, w = blockIdx.y;
   const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const size_t seg = (size_t)w * n;
@@ -295,7 +309,11 @@ __device__ __forceinline__ void sort_scatter_tile(const uint32_t *__restrict__ k
   }
   scan_256(tile_cnt, tile_off, warp_sums);
   for (unsigned d = threadIdx.x; d < SORT_RADIX; d += blockDim.x)
-    glob[d] = digit_base[(size_t)w * SORT_RADIX + d] + counts[((size_t)w * SORT_RADIX + d) * tiles + tile];
+    glob[d] = totals[(size_t)w * SORT_RADIX + d];
+  __syncthreads();
+  scan_256(glob, digit_base, warp_sums); // digit bases of this window
+  for (unsigned d = threadIdx.x; d < SORT_RADIX; d += blockDim.x)
+    glob[d] = digit_base[d] + counts[((size_t)w * SORT_RADIX + d) * tiles + tile];
 #pragma unroll
   for (unsigned r = 0; r < SORT_ITEMS; r++) {
     const unsigned i = sub + r * 32 + lane;
@@ -324,16 +342,16 @@ __global__ void __launch_bounds__(SORT_THREADS) sort_scatter_first_kernel(const 
                                                                           uint32_t *__restrict__ keys_out, uint32_t *__restrict__ vals_out,
                                                                           unsigned n, unsigned tiles, unsigned shift,
                                                                           const uint32_t *__restrict__ counts,
-                                                                          const uint32_t *__restrict__ digit_base) {
-  sort_scatter_tile<false>(keys_in, vals_in, keys_out, vals_out, n, tiles, shift, counts, digit_base);
+                                                                          const uint32_t *__restrict__ totals) {
+  sort_scatter_tile<false>(keys_in, vals_in, keys_out, vals_out, n, tiles, shift, counts, totals);
 }
 
 __global__ void __launch_bounds__(SORT_THREADS) sort_scatter_stable_kernel(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
                                                                            uint32_t *__restrict__ keys_out, uint32_t *__restrict__ vals_out,
                                                                            unsigned n, unsigned tiles, unsigned shift,
                                                                            const uint32_t *__restrict__ counts,
-                                                                           const uint32_t *__restrict__ digit_base) {
-  sort_scatter_tile<true>(keys_in, vals_in, keys_out, vals_out, n, tiles, shift, counts, digit_base);
+                                                                           const uint32_t *__restrict__ totals) {
+  sort_scatter_tile<true>(keys_in, vals_in, keys_out, vals_out, n, tiles, shift, counts, totals);
 }
 
 // ---------------------------------------------------------------------------
@@ -393,6 +411,15 @@ __device__ __forceinline__ affine signed_base(const affine *__restrict__ bases, 
   return p;
 }
 
+// 16-byte asynchronous global -> shared copies (L2 only: bases are not reused
+// by the same SM), one commit group per base point.
+__device__ __forceinline__ void cp_async_16(void *smem, const void *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int PENDING> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(PENDING) : "memory"); }
+
 __global__ void __launch_bounds__(ACC_THREADS, ACC_MIN_BLOCKS) accumulate_kernel(const uint32_t *__restrict__ keys, const uint32_t *__restrict__ vals,
                                                                  const affine *__restrict__ bases, unsigned n, unsigned windows, unsigned log_b,
                                                                  const uint32_t *__restrict__ zeros, unsigned total_threads,
@@ -400,6 +427,8 @@ __global__ void __launch_bounds__(ACC_THREADS, ACC_MIN_BLOCKS) accumulate_kernel
                                                                  uint32_t *__restrict__ head_bucket, xyzz *__restrict__ head_point) {
   __shared__ uint32_t s_zeros[MAX_WINDOWS];
   __shared__ unsigned long long s_prefix[MAX_WINDOWS + 1];
+  // two base-point slots per thread, chunk-major: [slot][16-byte chunk][thread]
+  __shared__ uint4 s_base[2][4][ACC_THREADS];
   for (unsigned w = threadIdx.x; w < windows; w += blockDim.x)
     s_zeros[w] = zeros[w];
   __syncthreads();
@@ -435,21 +464,75 @@ __global__ void __launch_bounds__(ACC_THREADS, ACC_MIN_BLOCKS) accumulate_kernel
   cur.idx = (size_t)w * n + s_zeros[w] + (size_t)(beg - s_prefix[w]);
   const uint32_t slot_mask = (1u << log_b) - 1;
 
+  auto issue = [&](unsigned slot, uint32_t val) {
+    const uint4 *src = reinterpret_cast<const uint4 *>(bases + (val & 0x7fffffffu));
+#pragma unroll
+    for (int c = 0; c < 4; c++)
+      cp_async_16(&s_base[slot][c][threadIdx.x], src + c);
+    cp_async_commit();
+  };
+  // A base's y is never 0 (BN254 G1 has odd order, so no point has y = 0):
+  // its negation is 2p - y.
+  auto fetch = [&](unsigned slot, uint32_t val) {
+    affine p;
+    uint32_t *w32 = reinterpret_cast<uint32_t *>(&p);
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      const uint4 v = s_base[slot][c][threadIdx.x];
+      w32[4 * c + 0] = v.x;
+      w32[4 * c + 1] = v.y;
+      w32[4 * c + 2] = v.z;
+      w32[4 * c + 3] = v.w;
+    }
+    const fe ny = fq::neg_nonzero(p.y);
+    const bool negative = val >> 31;
+#pragma unroll
+    for (int i = 0; i < 8; i++)
+      p.y.l[i] = negative ? ny.l[i] : p.y.l[i];
+    return p;
+  };
+
+  // entry 0 of the range
   uint32_t key = keys[cur.idx];
   uint32_t val = vals[cur.idx];
+  issue(0, val);
   // does this range start in the middle of a bucket?
   const bool continued = cur.idx > (size_t)w * n + s_zeros[w] && keys[cur.idx - 1] == key;
   unsigned bucket = (cur.w << log_b) | (key & slot_mask);
-  xyzz acc = curve::from_affine(signed_base(bases, val));
+  const unsigned long long count = end - beg;
+  // entry 1 is fetched before entry 0 is consumed
+  uint32_t nkey = 0, nval = 0;
+  unsigned nw = 0;
+  if (count > 1) {
+    cursor_advance(cur, n, windows, s_zeros);
+    nkey = keys[cur.idx];
+    nval = vals[cur.idx];
+    nw = cur.w;
+    issue(1, nval);
+    cp_async_wait<1>();
+  } else {
+    cp_async_wait<0>();
+  }
+  xyzz acc = curve::from_affine(fetch(0, val));
   bool acc_inf = false; // a partial sum can cancel to infinity (p + (-p))
   bool first = true;
-  const unsigned long long count = end - beg;
   for (unsigned long long k = 1; k < count; k++) {
-    cursor_advance(cur, n, windows, s_zeros);
-    key = keys[cur.idx];
-    val = vals[cur.idx];
-    const unsigned b = (cur.w << log_b) | (key & slot_mask);
-    const affine p = signed_base(bases, val);
+    key = nkey;
+    val = nval;
+    const unsigned kw = nw;
+    const unsigned slot = (unsigned)(k & 1);
+    if (k + 1 < count) {
+      cursor_advance(cur, n, windows, s_zeros);
+      nkey = keys[cur.idx];
+      nval = vals[cur.idx];
+      nw = cur.w;
+      issue(slot ^ 1, nval);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    const affine p = fetch(slot, val);
+    const unsigned b = (kw << log_b) | (key & slot_mask);
     if (b != bucket) {
       if (acc_inf)
         acc = curve::infinity();

@@ -70,20 +70,23 @@ struct plan {
 // and the top window of a W*c >= 254 split never carries out.
 __global__ void digits_kernel(const fe *__restrict__ scalars, unsigned n, unsigned c, unsigned windows, uint32_t *__restrict__ keys,
                               uint32_t *__restrict__ vals);
+// the same, also writing the first radix pass's tile histograms
+__global__ void digits_histogram_kernel(const fe *__restrict__ scalars, unsigned n, unsigned c, unsigned windows, unsigned tiles,
+                                        uint32_t *__restrict__ keys, uint32_t *__restrict__ vals, uint32_t *__restrict__ counts);
 
 // ---------------------------------------------------------------------------
 // 2. sort (keys and values per window segment of n entries)
 // ---------------------------------------------------------------------------
 __global__ void sort_histogram_kernel(const uint32_t *__restrict__ keys, unsigned n, unsigned tiles, unsigned shift,
                                       uint32_t *__restrict__ counts);
-__global__ void sort_scan_kernel(uint32_t *counts, unsigned tiles, uint32_t *__restrict__ digit_base);
+__global__ void sort_scan_kernel(uint32_t *counts, unsigned tiles, unsigned rows, uint32_t *__restrict__ totals);
 // first pass (any order among equal digits) and later passes (stable)
 __global__ void sort_scatter_first_kernel(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in, uint32_t *__restrict__ keys_out,
                                           uint32_t *__restrict__ vals_out, unsigned n, unsigned tiles, unsigned shift,
-                                          const uint32_t *__restrict__ counts, const uint32_t *__restrict__ digit_base);
+                                          const uint32_t *__restrict__ counts, const uint32_t *__restrict__ totals);
 __global__ void sort_scatter_stable_kernel(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in, uint32_t *__restrict__ keys_out,
                                            uint32_t *__restrict__ vals_out, unsigned n, unsigned tiles, unsigned shift,
-                                           const uint32_t *__restrict__ counts, const uint32_t *__restrict__ digit_base);
+                                           const uint32_t *__restrict__ counts, const uint32_t *__restrict__ totals);
 
 // ---------------------------------------------------------------------------
 // 3. zero counts
