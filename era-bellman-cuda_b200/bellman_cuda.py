@@ -31,6 +31,10 @@ BC_ERROR_INVALID_VALUE = 1
 BC_ERROR_MEMORY_ALLOCATION = 2
 BC_ERROR_NOT_READY = 600
 
+# msm_b200_execute_no_alloc_async limits (include/bellman-cuda-b200.h)
+NO_ALLOC_MAX_COUNT = 65536
+NO_ALLOC_SCRATCH_BYTES = 64 << 20
+
 
 class BcError(RuntimeError):
     def __init__(self, code: int, what: str):
@@ -172,6 +176,7 @@ class BellmanCuda:
                 "msm_b200_execute_staged_async": [ctypes.POINTER(MsmB200Configuration), ctypes.POINTER(Handle),
                                                   ctypes.POINTER(ctypes.c_uint)],
                 "msm_b200_measure_mul_throughput": [u, ctypes.POINTER(ctypes.c_double)],
+                "msm_b200_execute_no_alloc_async": [Handle, vp, vp, vp, u],
             }
             for name, args in ext.items():
                 f = getattr(L, name)
@@ -356,6 +361,10 @@ class BellmanCuda:
         b = ctypes.c_size_t()
         self.check(self.lib.msm_b200_scratch_bytes(count, window_bits, ctypes.byref(b)), "msm_b200_scratch_bytes")
         return b.value
+
+    def msm_no_alloc(self, stream: Handle, bases, scalars, results, count: int) -> int:
+        """msm_b200_execute_no_alloc_async: device buffers only, count <= NO_ALLOC_MAX_COUNT; returns the bc_error."""
+        return self.lib.msm_b200_execute_no_alloc_async(stream, _ptr(bases), _ptr(scalars), _ptr(results), count)
 
     def default_window_bits(self, count: int) -> int:
         c = ctypes.c_uint()

@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
+#include <initializer_list>
 #include <mutex>
 #include <vector>
 
@@ -404,6 +405,55 @@ cudaError_t set_up() {
   return cudaSuccess;
 }
 
+// ---------------------------------------------------------------------------
+// MSM without allocation: scratch in a fixed block of device memory that is
+// part of the library image, for callers that cannot allocate at call time.
+// ---------------------------------------------------------------------------
+static_assert(MSM_B200_NO_ALLOC_SCRATCH_BYTES % 256 == 0, "scratch block size");
+static __device__ __align__(256) uint8_t no_alloc_scratch[MSM_B200_NO_ALLOC_SCRATCH_BYTES];
+
+// Device address of no_alloc_scratch on `device` (the current device).  In
+// host code the symbol is only a host-side handle; the address comes from
+// cudaGetSymbolAddress, looked up once per device and cached.
+static cudaError_t no_alloc_scratch_address(int device, uint8_t **address) {
+  static std::mutex lock;
+  static uint8_t *cache[64] = {};
+  if (device < 0 || device >= 64)
+    return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> guard(lock);
+  if (!cache[device]) {
+    void *ptr = nullptr;
+    CHECK(cudaGetSymbolAddress(&ptr, no_alloc_scratch));
+    cache[device] = static_cast<uint8_t *>(ptr);
+  }
+  *address = cache[device];
+  return cudaSuccess;
+}
+
+cudaError_t execute_no_alloc(cudaStream_t stream, const void *bases, const void *scalars, void *results, unsigned count) {
+  if (count == 0 || count > MSM_B200_NO_ALLOC_MAX_COUNT || !bases || !scalars || !results)
+    return cudaErrorInvalidValue;
+  if ((reinterpret_cast<uintptr_t>(bases) & 15) || (reinterpret_cast<uintptr_t>(scalars) & 15) || (reinterpret_cast<uintptr_t>(results) & 15))
+    return cudaErrorInvalidValue;
+  cudaError_t err;
+  for (const void *ptr : {bases, scalars, static_cast<const void *>(results)}) {
+    const bool host = is_host_pointer(ptr, err);
+    CHECK(err);
+    if (host)
+      return cudaErrorInvalidValue;
+  }
+  int device = 0;
+  CHECK(cudaGetDevice(&device));
+  const plan p = make_plan(count, 0, get_device_info(device).sms);
+  const layout l = make_layout(p, false, false, false);
+  if (l.total > MSM_B200_NO_ALLOC_SCRATCH_BYTES) // only on GPUs far larger than a B200 (heads grow with the SM count)
+    return cudaErrorInvalidValue;
+  uint8_t *scratch = nullptr;
+  CHECK(no_alloc_scratch_address(device, &scratch));
+  return enqueue_pipeline(p, static_cast<const fe *>(scalars), static_cast<const affine *>(bases), static_cast<jacobian *>(results), scratch, l,
+                          stream);
+}
+
 } // namespace msm_b200
 
 // ---------------------------------------------------------------------------
@@ -495,6 +545,10 @@ bc_error msm_b200_default_window_bits(unsigned count, unsigned *window_bits) {
     return bc_error_invalid_value;
   *window_bits = msm_b200::default_window_bits(count);
   return bc_success;
+}
+
+bc_error msm_b200_execute_no_alloc_async(bc_stream stream, const void *bases, const void *scalars, void *results, unsigned count) {
+  return static_cast<bc_error>(msm_b200::execute_no_alloc(static_cast<cudaStream_t>(stream.handle), bases, scalars, results, count));
 }
 
 } // extern "C"

@@ -72,6 +72,34 @@ bc_error msm_b200_default_window_bits(unsigned count, unsigned *window_bits);
  * memory.  Used to build synthetic base tables on the device. */
 bc_error msm_b200_generator_multiples_async(const void *k, void *bases, unsigned count, bc_stream stream);
 
+/* An MSM that allocates no memory (no counterpart in the reference).
+ *
+ * For callers that cannot allocate device memory at call time: code running
+ * inside a host callback or a driver/loader layer where cudaMalloc is not
+ * allowed, a prover whose device memory is pre-committed by its own
+ * allocator, or a process that must not grow its footprint after start-up.
+ * Every other MSM entry point takes its scratch from a memory pool on every
+ * call; this one uses a fixed block of device memory that is part of the
+ * library image (MSM_B200_NO_ALLOC_SCRATCH_BYTES, 64 MiB), which every GPU
+ * that loads the library holds until the process exits.
+ *
+ * bases, scalars and results must all be device memory (nothing is copied
+ * in or out); layout and result convention as msm_execute_async, with any
+ * count in [1, MSM_B200_NO_ALLOC_MAX_COUNT].  A count outside that range, a
+ * null or host pointer, or a misaligned buffer returns bc_error_invalid_value
+ * before anything is enqueued.  The window width is the size-based default.
+ *
+ * The first call on a device looks up the block's device address (once per
+ * device, with that device current); make that first call before any stream
+ * capture.  Every call shares the one block and the block keeps the last
+ * call's contents (whatever must start at zero is cleared by each call): two
+ * calls whose work overlaps on the GPU, on different streams or from
+ * different threads, race and both results are undefined.  Serialise them,
+ * e.g. on one stream. */
+#define MSM_B200_NO_ALLOC_MAX_COUNT 65536u
+#define MSM_B200_NO_ALLOC_SCRATCH_BYTES (64u << 20)
+bc_error msm_b200_execute_no_alloc_async(bc_stream stream, const void *bases, const void *scalars, void *results, unsigned count);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif
