@@ -87,14 +87,63 @@ plan make_plan(unsigned n, unsigned window_bits, int sms) {
   return p;
 }
 
-// Scratch layout inside one pool allocation.
+// Host-resident inputs are processed in chunks of points: the copy of chunk
+// j + 1 runs on a helper stream while chunk j is sorted and accumulated, and
+// every chunk after the first accumulates into its own buckets, which are then
+// folded into the MSM's.  Chunk sizes grow by CHUNK_GROWTH (the pipeline takes
+// about five times as long per point as the host-to-device copy), so only the
+// first, small chunk's copy is exposed.  Reference counterpart: the chunked
+// copy/compute overlap of schedule_execution (src/msm.cu:160-334).
+constexpr unsigned MAX_CHUNKS = 4;
+constexpr unsigned CHUNK_GROWTH = 4;
+constexpr unsigned MIN_FIRST_CHUNK = 1u << 16;
+
+struct chunking {
+  unsigned count = 1;
+  unsigned beg[MAX_CHUNKS + 1] = {};
+};
+
+static chunking make_chunks(unsigned n, bool copy_inputs) {
+  chunking ch;
+  unsigned k = 1;
+  if (copy_inputs) {
+    // largest k <= MAX_CHUNKS whose first chunk n / (1 + 4 + ... + 4^(k-1)) is >= MIN_FIRST_CHUNK
+    unsigned long long weight = 1, total = 1;
+    while (k < MAX_CHUNKS) {
+      const unsigned long long next_total = total + weight * CHUNK_GROWTH;
+      if ((unsigned long long)n < MIN_FIRST_CHUNK * next_total)
+        break;
+      weight *= CHUNK_GROWTH;
+      total = next_total;
+      k++;
+    }
+  }
+  ch.count = k;
+  unsigned long long total = 0, weight = 1;
+  for (unsigned j = 0; j < k; j++, weight *= CHUNK_GROWTH)
+    total += weight;
+  unsigned long long acc = 0;
+  weight = 1;
+  for (unsigned j = 0; j < k; j++, weight *= CHUNK_GROWTH) {
+    ch.beg[j] = (unsigned)((unsigned long long)n * acc / total);
+    acc += weight;
+  }
+  ch.beg[k] = n;
+  return ch;
+}
+
+// Scratch layout inside one pool allocation.  `p` is the plan of the largest
+// chunk (keys, values and heads are reused chunk after chunk); copies of
+// host-resident inputs are sized for all `copy_n` points; a chunked MSM holds a
+// second bucket set for the chunks after the first.
 struct layout {
-  size_t keys[2], vals[2], counts, totals, zeros, buckets, flags, hb[2], hp[2], tree[2], streams[2], results, scalars, bases, total;
+  size_t keys[2], vals[2], counts, totals, zeros, buckets, flags, chunk_buckets, chunk_flags, hb[2], hp[2], tree[2], streams[2], results,
+      scalars, bases, total;
 };
 
 static size_t align_up(size_t v) { return (v + 255) & ~(size_t)255; }
 
-static layout make_layout(const plan &p, bool copy_scalars, bool copy_bases, bool copy_results) {
+static layout make_layout(const plan &p, bool copy_scalars, bool copy_bases, bool copy_results, unsigned copy_n = 0, bool chunked = false) {
   layout l{};
   size_t off = 0;
   auto take = [&](size_t bytes) {
@@ -102,6 +151,8 @@ static layout make_layout(const plan &p, bool copy_scalars, bool copy_bases, boo
     off += align_up(bytes);
     return at;
   };
+  if (!copy_n)
+    copy_n = p.n;
   const size_t entries = (size_t)p.windows * p.n;
   for (int i = 0; i < 2; i++) {
     l.keys[i] = take(entries * 4);
@@ -113,6 +164,10 @@ static layout make_layout(const plan &p, bool copy_scalars, bool copy_bases, boo
   const size_t slots = (size_t)p.windows << p.log_b;
   l.buckets = take(slots * sizeof(xyzz));
   l.flags = take(slots);
+  if (chunked) {
+    l.chunk_buckets = take(slots * sizeof(xyzz));
+    l.chunk_flags = take(slots);
+  }
   for (int i = 0; i < 2; i++) {
     l.hb[i] = take((size_t)p.acc_threads * 4);
     l.hp[i] = take((size_t)p.acc_threads * sizeof(xyzz));
@@ -122,17 +177,28 @@ static layout make_layout(const plan &p, bool copy_scalars, bool copy_bases, boo
     l.streams[i] = take((size_t)p.windows * stream_stride(p.log_g) * sizeof(xyzz));
   }
   l.results = copy_results ? take(RESULT_BITS * sizeof(jacobian)) : 0;
-  l.scalars = copy_scalars ? take((size_t)p.n * sizeof(fe)) : 0;
-  l.bases = copy_bases ? take((size_t)p.n * sizeof(affine)) : 0;
+  l.scalars = copy_scalars ? take((size_t)copy_n * sizeof(fe)) : 0;
+  l.bases = copy_bases ? take((size_t)copy_n * sizeof(affine)) : 0;
   l.total = off;
   return l;
+}
+
+// Plan of the largest chunk of an n-point MSM split as `ch`, at the window
+// width of the whole MSM.
+static plan largest_chunk_plan(unsigned n, unsigned window_bits, int sms, const chunking &ch) {
+  const unsigned c = window_bits ? window_bits : default_window_bits(n);
+  unsigned largest = 0;
+  for (unsigned j = 0; j < ch.count; j++)
+    largest = std::max(largest, ch.beg[j + 1] - ch.beg[j]);
+  return make_plan(largest, c, sms);
 }
 
 size_t scratch_bytes(unsigned n, unsigned window_bits, bool copy_scalars, bool copy_bases, bool copy_results) {
   int device = 0;
   cudaGetDevice(&device);
-  const plan p = make_plan(n, window_bits, get_device_info(device).sms);
-  return make_layout(p, copy_scalars, copy_bases, copy_results).total;
+  const chunking ch = make_chunks(n, copy_scalars || copy_bases);
+  const plan p = largest_chunk_plan(n, window_bits, get_device_info(device).sms, ch);
+  return make_layout(p, copy_scalars, copy_bases, copy_results, n, ch.count > 1).total;
 }
 
 static bool is_host_pointer(const void *ptr, cudaError_t &err) {
@@ -143,26 +209,27 @@ static bool is_host_pointer(const void *ptr, cudaError_t &err) {
   return attr.type == cudaMemoryTypeUnregistered || attr.type == cudaMemoryTypeHost;
 }
 
-// Enqueue the kernels of one MSM whose inputs are on the device.
-// stage_events (optional): PROFILE_STAGES + 1 events recorded before the first
-// stage and after each stage.  launches (optional): kernels enqueued.
-cudaError_t enqueue_pipeline(const plan &p, const fe *scalars, const affine *bases, jacobian *results, uint8_t *scratch, const layout &l,
-                             cudaStream_t stream, cudaEvent_t *stage_events = nullptr, unsigned *launches = nullptr) {
+// Stage boundaries: optional caller events recorded before the first stage and
+// after each of the PROFILE_STAGES stages, and a count of kernels enqueued.
+struct stage_marks {
+  cudaEvent_t *events = nullptr;
+  unsigned next = 0;
   unsigned launched = 0;
-  unsigned stage = 0;
-  auto mark = [&]() -> cudaError_t { return stage_events ? cudaEventRecord(stage_events[stage++], stream) : cudaSuccess; };
-  CHECK(mark());
+  cudaError_t mark(cudaStream_t stream) { return events ? cudaEventRecord(events[next++], stream) : cudaSuccess; }
+};
+
+// Stages 1-5 for the points of one plan: digits, sort, zero counts,
+// accumulation and head merge into (buckets, flags).  Flags must be zero for
+// buckets that hold nothing yet.
+static cudaError_t enqueue_accumulation(const plan &p, const fe *scalars, const affine *bases, xyzz *buckets, uint8_t *flags, uint8_t *scratch,
+                                        const layout &l, cudaStream_t stream, stage_marks &m) {
   uint32_t *keys[2] = {reinterpret_cast<uint32_t *>(scratch + l.keys[0]), reinterpret_cast<uint32_t *>(scratch + l.keys[1])};
   uint32_t *vals[2] = {reinterpret_cast<uint32_t *>(scratch + l.vals[0]), reinterpret_cast<uint32_t *>(scratch + l.vals[1])};
   uint32_t *counts = reinterpret_cast<uint32_t *>(scratch + l.counts);
   uint32_t *totals = reinterpret_cast<uint32_t *>(scratch + l.totals);
   uint32_t *zeros = reinterpret_cast<uint32_t *>(scratch + l.zeros);
-  xyzz *buckets = reinterpret_cast<xyzz *>(scratch + l.buckets);
-  uint8_t *flags = scratch + l.flags;
   uint32_t *hb[2] = {reinterpret_cast<uint32_t *>(scratch + l.hb[0]), reinterpret_cast<uint32_t *>(scratch + l.hb[1])};
   xyzz *hp[2] = {reinterpret_cast<xyzz *>(scratch + l.hp[0]), reinterpret_cast<xyzz *>(scratch + l.hp[1])};
-  xyzz *tree[2] = {reinterpret_cast<xyzz *>(scratch + l.tree[0]), reinterpret_cast<xyzz *>(scratch + l.tree[1])};
-  xyzz *streams[2] = {reinterpret_cast<xyzz *>(scratch + l.streams[0]), reinterpret_cast<xyzz *>(scratch + l.streams[1])};
   const unsigned n = p.n;
 
   // 1. digits (with the first sort pass's histograms when they fit in shared memory)
@@ -174,8 +241,8 @@ cudaError_t enqueue_pipeline(const plan &p, const fe *scalars, const affine *bas
     digits_kernel<<<(n + 255) / 256, 256, 0, stream>>>(scalars, n, p.c, p.windows, keys[0], vals[0]);
   }
   CHECK(cudaGetLastError());
-  launched++;
-  CHECK(mark());
+  m.launched++;
+  CHECK(m.mark(stream));
 
   // 2. sort, 8 bits per pass
   int cur = 0;
@@ -186,7 +253,7 @@ cudaError_t enqueue_pipeline(const plan &p, const fe *scalars, const affine *bas
     if (pass > 0 || !fused_histogram) {
       sort_histogram_kernel<<<grid, SORT_THREADS, 0, stream>>>(keys[cur], n, p.tiles, shift, counts);
       CHECK(cudaGetLastError());
-      launched++;
+      m.launched++;
     }
     sort_scan_kernel<<<(rows * 32 + 255) / 256, 256, 0, stream>>>(counts, p.tiles, rows, totals);
     CHECK(cudaGetLastError());
@@ -197,24 +264,23 @@ cudaError_t enqueue_pipeline(const plan &p, const fe *scalars, const affine *bas
       sort_scatter_stable_kernel<<<grid, SORT_THREADS, 0, stream>>>(keys[cur], vals[cur], keys[cur ^ 1], vals[cur ^ 1], n, p.tiles, shift, counts,
                                                                     totals);
     CHECK(cudaGetLastError());
-    launched += 2;
+    m.launched += 2;
     cur ^= 1;
   }
-  CHECK(mark());
+  CHECK(m.mark(stream));
 
   // 3. zero-digit prefix of every window
   zero_counts_kernel<<<(p.windows + 127) / 128, 128, 0, stream>>>(keys[cur], n, p.windows, zeros);
   CHECK(cudaGetLastError());
-  launched++;
-  CHECK(cudaMemsetAsync(flags, 0, (size_t)p.windows << p.log_b, stream));
-  CHECK(mark());
+  m.launched++;
+  CHECK(m.mark(stream));
 
   // 4. accumulation
   accumulate_kernel<<<(p.acc_threads + ACC_THREADS - 1) / ACC_THREADS, ACC_THREADS, 0, stream>>>(
       keys[cur], vals[cur], bases, n, p.windows, p.log_b, zeros, p.acc_threads, buckets, flags, hb[0], hp[0]);
   CHECK(cudaGetLastError());
-  launched++;
-  CHECK(mark());
+  m.launched++;
+  CHECK(m.mark(stream));
 
   // 5. heads
   unsigned heads = p.acc_threads;
@@ -224,25 +290,31 @@ cudaError_t enqueue_pipeline(const plan &p, const fe *scalars, const affine *bas
     merge_heads_kernel<<<(out + ACC_THREADS - 1) / ACC_THREADS, ACC_THREADS, 0, stream>>>(hb[h], hp[h], heads, p.merge_chunk, buckets,
                                                                                            hb[h ^ 1], hp[h ^ 1]);
     CHECK(cudaGetLastError());
-    launched++;
+    m.launched++;
     heads = out;
     h ^= 1;
   }
-  CHECK(mark());
+  CHECK(m.mark(stream));
+  return cudaSuccess;
+}
 
-  // 6. reduction
+// Stage 6: bucket reduction of (buckets, flags) into the 254 results.
+static cudaError_t enqueue_reduction(const plan &p, const xyzz *buckets, const uint8_t *flags, jacobian *results, uint8_t *scratch, const layout &l,
+                                     cudaStream_t stream, stage_marks &m) {
+  xyzz *tree[2] = {reinterpret_cast<xyzz *>(scratch + l.tree[0]), reinterpret_cast<xyzz *>(scratch + l.tree[1])};
+  xyzz *streams[2] = {reinterpret_cast<xyzz *>(scratch + l.streams[0]), reinterpret_cast<xyzz *>(scratch + l.streams[1])};
   const unsigned group_threads = p.windows << p.log_g;
   reduce_groups_kernel<<<(group_threads + ACC_THREADS - 1) / ACC_THREADS, ACC_THREADS, 0, stream>>>(buckets, flags, p.windows, p.log_b,
                                                                                                      p.log_m, tree[0], streams[0]);
   CHECK(cudaGetLastError());
-  launched++;
+  m.launched++;
   int t = 0;
   for (unsigned level = 0; level < p.log_g; level++) {
     const unsigned threads = p.windows * ((1u << p.log_g) >> (level + 1));
     reduce_tree_kernel<<<(threads + ACC_THREADS - 1) / ACC_THREADS, ACC_THREADS, 0, stream>>>(tree[t], tree[t ^ 1], streams[0], p.windows,
                                                                                                p.log_g, level);
     CHECK(cudaGetLastError());
-    launched++;
+    m.launched++;
     t ^= 1;
   }
   int s = 0;
@@ -252,17 +324,33 @@ cudaError_t enqueue_pipeline(const plan &p, const fe *scalars, const affine *bas
     const dim3 grid((len_out + ACC_THREADS - 1) / ACC_THREADS, p.windows * (p.log_g + 1));
     reduce_streams_kernel<<<grid, ACC_THREADS, 0, stream>>>(streams[s], streams[s ^ 1], p.windows, p.log_g, p.sum_fanin, divisor);
     CHECK(cudaGetLastError());
-    launched++;
+    m.launched++;
     divisor *= p.sum_fanin;
     s ^= 1;
   }
   gather_results_kernel<<<(RESULT_BITS + 127) / 128, 128, 0, stream>>>(streams[s], buckets, flags, p.windows, p.c, p.log_m, p.log_g,
                                                                        divisor, results);
   CHECK(cudaGetLastError());
-  launched++;
-  CHECK(mark());
+  m.launched++;
+  CHECK(m.mark(stream));
+  return cudaSuccess;
+}
+
+// Enqueue the kernels of one MSM whose inputs are on the device.
+// stage_events (optional): PROFILE_STAGES + 1 events recorded before the first
+// stage and after each stage.  launches (optional): kernels enqueued.
+cudaError_t enqueue_pipeline(const plan &p, const fe *scalars, const affine *bases, jacobian *results, uint8_t *scratch, const layout &l,
+                             cudaStream_t stream, cudaEvent_t *stage_events = nullptr, unsigned *launches = nullptr) {
+  stage_marks m;
+  m.events = stage_events;
+  xyzz *buckets = reinterpret_cast<xyzz *>(scratch + l.buckets);
+  uint8_t *flags = scratch + l.flags;
+  CHECK(cudaMemsetAsync(flags, 0, (size_t)p.windows << p.log_b, stream));
+  CHECK(m.mark(stream));
+  CHECK(enqueue_accumulation(p, scalars, bases, buckets, flags, scratch, l, stream, m));
+  CHECK(enqueue_reduction(p, buckets, flags, results, scratch, l, stream, m));
   if (launches)
-    *launches = launched;
+    *launches = m.launched;
   return cudaSuccess;
 }
 
@@ -297,6 +385,92 @@ static cudaError_t collect_profile(const plan &p, const layout &l, const uint8_t
   return cudaSuccess;
 }
 
+// Events and the helper stream of a chunked MSM, released when the call ends
+// (the CUDA runtime defers the release of a stream or event until its pending
+// work completes).
+struct chunk_resources {
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ready = nullptr, copied[MAX_CHUNKS] = {}, copies_done = nullptr;
+  ~chunk_resources() {
+    for (cudaEvent_t e : copied)
+      if (e)
+        cudaEventDestroy(e);
+    if (ready)
+      cudaEventDestroy(ready);
+    if (copies_done)
+      cudaEventDestroy(copies_done);
+    if (copy_stream)
+      cudaStreamDestroy(copy_stream);
+  }
+};
+
+// A chunked MSM over host-resident scalars and/or bases (see make_chunks).
+static cudaError_t enqueue_chunked(const execution &e, const chunking &ch, const plan &full, unsigned sms, bool copy_scalars, bool copy_bases,
+                                   jacobian *device_results, uint8_t *scratch, const layout &l) {
+  cudaStream_t stream = e.stream;
+  chunk_resources r;
+  CHECK(cudaStreamCreateWithFlags(&r.copy_stream, cudaStreamNonBlocking));
+  CHECK(cudaEventCreateWithFlags(&r.ready, cudaEventDisableTiming));
+  CHECK(cudaEventCreateWithFlags(&r.copies_done, cudaEventDisableTiming));
+  for (unsigned j = 0; j < ch.count; j++)
+    CHECK(cudaEventCreateWithFlags(&r.copied[j], cudaEventDisableTiming));
+  // the copies go into scratch allocated in the caller's stream order
+  CHECK(cudaEventRecord(r.ready, stream));
+  CHECK(cudaStreamWaitEvent(r.copy_stream, r.ready, 0));
+  fe *scalars = reinterpret_cast<fe *>(scratch + l.scalars);
+  affine *bases = reinterpret_cast<affine *>(scratch + l.bases);
+  auto enqueue_copy = [&](unsigned j) -> cudaError_t {
+    const unsigned b = ch.beg[j], cnt = ch.beg[j + 1] - b;
+    if (copy_scalars)
+      CHECK(cudaMemcpyAsync(scalars + b, static_cast<const fe *>(e.scalars) + b, (size_t)cnt * sizeof(fe), cudaMemcpyHostToDevice, r.copy_stream));
+    if (copy_bases)
+      CHECK(cudaMemcpyAsync(bases + b, static_cast<const affine *>(e.bases) + b, (size_t)cnt * sizeof(affine), cudaMemcpyHostToDevice,
+                            r.copy_stream));
+    CHECK(cudaEventRecord(r.copied[j], r.copy_stream));
+    if (j + 1 == ch.count) {
+      if (e.h2d_event)
+        CHECK(cudaEventRecord(e.h2d_event, r.copy_stream));
+      if (e.h2d_callback)
+        CHECK(cudaLaunchHostFunc(r.copy_stream, e.h2d_callback, e.h2d_callback_data));
+      CHECK(cudaEventRecord(r.copies_done, r.copy_stream));
+    }
+    return cudaSuccess;
+  };
+
+  const fe *src_scalars = copy_scalars ? scalars : static_cast<const fe *>(e.scalars);
+  const affine *src_bases = copy_bases ? bases : static_cast<const affine *>(e.bases);
+  xyzz *buckets = reinterpret_cast<xyzz *>(scratch + l.buckets);
+  uint8_t *flags = scratch + l.flags;
+  xyzz *chunk_buckets = reinterpret_cast<xyzz *>(scratch + l.chunk_buckets);
+  uint8_t *chunk_flags = scratch + l.chunk_flags;
+  const size_t slots = (size_t)full.windows << full.log_b;
+  stage_marks m;
+  CHECK(cudaMemsetAsync(flags, 0, slots, stream));
+  // copy j + 1 is enqueued before chunk j's kernels, so that the host thread
+  // (which stages pageable copies itself) never holds back enqueued work
+  CHECK(enqueue_copy(0));
+  for (unsigned j = 0; j < ch.count; j++) {
+    if (j + 1 < ch.count)
+      CHECK(enqueue_copy(j + 1));
+    const unsigned b = ch.beg[j];
+    const plan p = make_plan(ch.beg[j + 1] - b, full.c, sms);
+    CHECK(cudaStreamWaitEvent(stream, r.copied[j], 0));
+    if (j == 0) {
+      CHECK(enqueue_accumulation(p, src_scalars + b, src_bases + b, buckets, flags, scratch, l, stream, m));
+    } else {
+      CHECK(cudaMemsetAsync(chunk_flags, 0, slots, stream));
+      CHECK(enqueue_accumulation(p, src_scalars + b, src_bases + b, chunk_buckets, chunk_flags, scratch, l, stream, m));
+      merge_chunk_buckets_kernel<<<(unsigned)((slots + ACC_THREADS - 1) / ACC_THREADS), ACC_THREADS, 0, stream>>>(buckets, flags, chunk_buckets,
+                                                                                                                 chunk_flags, (unsigned)slots);
+      CHECK(cudaGetLastError());
+    }
+  }
+  CHECK(enqueue_reduction(full, buckets, flags, device_results, scratch, l, stream, m));
+  // the call's stream completes after the copies and the h2d callback
+  CHECK(cudaStreamWaitEvent(stream, r.copies_done, 0));
+  return cudaSuccess;
+}
+
 cudaError_t execute(const execution &e) {
   if (e.count == 0 || e.count > (1u << 31) || !e.scalars || !e.bases || !e.results)
     return cudaErrorInvalidValue;
@@ -313,10 +487,14 @@ cudaError_t execute(const execution &e) {
   CHECK(err);
   const bool copy_results = is_host_pointer(e.results, err);
   CHECK(err);
-  const plan p = make_plan(e.count, e.window_bits, get_device_info(device).sms);
+  const int sms = get_device_info(device).sms;
+  const bool instrumented = e.profile || e.stage_events;
+  const chunking ch = make_chunks(e.count, (copy_scalars || copy_bases) && !instrumented);
+  const plan p = make_plan(e.count, e.window_bits, sms);
   if (p.windows > 128)
     return cudaErrorInvalidValue;
-  const layout l = make_layout(p, copy_scalars, copy_bases, copy_results);
+  const plan largest = ch.count > 1 ? largest_chunk_plan(e.count, p.c, sms, ch) : p;
+  const layout l = make_layout(largest, copy_scalars, copy_bases, copy_results, e.count, ch.count > 1);
   cudaStream_t stream = e.stream;
   void *raw = nullptr;
   if (e.pool)
@@ -329,46 +507,51 @@ cudaError_t execute(const execution &e) {
     const fe *scalars = static_cast<const fe *>(e.scalars);
     const affine *bases = static_cast<const affine *>(e.bases);
     jacobian *results = static_cast<jacobian *>(e.results);
-    if (copy_scalars) {
-      if ((status = cudaMemcpyAsync(scratch + l.scalars, e.scalars, (size_t)p.n * sizeof(fe), cudaMemcpyHostToDevice, stream)) != cudaSuccess)
-        break;
-      scalars = reinterpret_cast<const fe *>(scratch + l.scalars);
-    }
-    if (copy_bases) {
-      if ((status = cudaMemcpyAsync(scratch + l.bases, e.bases, (size_t)p.n * sizeof(affine), cudaMemcpyHostToDevice, stream)) != cudaSuccess)
-        break;
-      bases = reinterpret_cast<const affine *>(scratch + l.bases);
-    }
-    if (copy_scalars || copy_bases) {
-      if (e.h2d_event && (status = cudaEventRecord(e.h2d_event, stream)) != cudaSuccess)
-        break;
-      if (e.h2d_callback && (status = cudaLaunchHostFunc(stream, e.h2d_callback, e.h2d_callback_data)) != cudaSuccess)
-        break;
-    }
     jacobian *device_results = copy_results ? reinterpret_cast<jacobian *>(scratch + l.results) : results;
-    cudaEvent_t events[PROFILE_STAGES + 1] = {};
-    const cudaEvent_t *stage_events = e.stage_events;
-    if (e.profile) {
-      for (auto &ev : events)
-        if ((status = cudaEventCreate(&ev)) != cudaSuccess)
+    if (ch.count > 1) {
+      if ((status = enqueue_chunked(e, ch, p, sms, copy_scalars, copy_bases, device_results, scratch, l)) != cudaSuccess)
+        break;
+    } else {
+      if (copy_scalars) {
+        if ((status = cudaMemcpyAsync(scratch + l.scalars, e.scalars, (size_t)p.n * sizeof(fe), cudaMemcpyHostToDevice, stream)) != cudaSuccess)
           break;
-      if (status != cudaSuccess)
+        scalars = reinterpret_cast<const fe *>(scratch + l.scalars);
+      }
+      if (copy_bases) {
+        if ((status = cudaMemcpyAsync(scratch + l.bases, e.bases, (size_t)p.n * sizeof(affine), cudaMemcpyHostToDevice, stream)) != cudaSuccess)
+          break;
+        bases = reinterpret_cast<const affine *>(scratch + l.bases);
+      }
+      if (copy_scalars || copy_bases) {
+        if (e.h2d_event && (status = cudaEventRecord(e.h2d_event, stream)) != cudaSuccess)
+          break;
+        if (e.h2d_callback && (status = cudaLaunchHostFunc(stream, e.h2d_callback, e.h2d_callback_data)) != cudaSuccess)
+          break;
+      }
+      cudaEvent_t events[PROFILE_STAGES + 1] = {};
+      const cudaEvent_t *stage_events = e.stage_events;
+      if (e.profile) {
+        for (auto &ev : events)
+          if ((status = cudaEventCreate(&ev)) != cudaSuccess)
+            break;
+        if (status != cudaSuccess)
+          break;
+      }
+      unsigned launches = 0;
+      if (e.profile)
+        stage_events = events;
+      if ((status = enqueue_pipeline(p, scalars, bases, device_results, scratch, l, stream, const_cast<cudaEvent_t *>(stage_events), &launches)) !=
+          cudaSuccess)
         break;
-    }
-    unsigned launches = 0;
-    if (e.profile)
-      stage_events = events;
-    if ((status = enqueue_pipeline(p, scalars, bases, device_results, scratch, l, stream, const_cast<cudaEvent_t *>(stage_events), &launches)) !=
-        cudaSuccess)
-      break;
-    if (e.launches)
-      *e.launches = launches;
-    if (e.profile) {
-      status = collect_profile(p, l, scratch, stream, events, launches, e.profile);
-      for (auto &ev : events)
-        cudaEventDestroy(ev);
-      if (status != cudaSuccess)
-        break;
+      if (e.launches)
+        *e.launches = launches;
+      if (e.profile) {
+        status = collect_profile(p, l, scratch, stream, events, launches, e.profile);
+        for (auto &ev : events)
+          cudaEventDestroy(ev);
+        if (status != cudaSuccess)
+          break;
+      }
     }
     if (copy_results) {
       if ((status = cudaMemcpyAsync(e.results, device_results, RESULT_BITS * sizeof(jacobian), cudaMemcpyDeviceToHost, stream)) != cudaSuccess)

@@ -612,6 +612,20 @@ __global__ void __launch_bounds__(ACC_THREADS) merge_heads_kernel(const uint32_t
   }
 }
 
+// Fold the buckets of one chunk of points into the MSM's buckets (host-resident
+// inputs are processed in chunks whose copies overlap the previous chunk's
+// work).  One thread per bucket slot.
+__global__ void __launch_bounds__(ACC_THREADS) merge_chunk_buckets_kernel(xyzz *__restrict__ buckets, uint8_t *__restrict__ flags,
+                                                                          const xyzz *__restrict__ chunk_buckets,
+                                                                          const uint8_t *__restrict__ chunk_flags, unsigned slots) {
+  const unsigned b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= slots || !chunk_flags[b])
+    return;
+  const xyzz q = load_xyzz(chunk_buckets + b);
+  store_xyzz(buckets + b, flags[b] ? curve::add(load_xyzz(buckets + b), q) : q);
+  flags[b] = 1;
+}
+
 // ---------------------------------------------------------------------------
 // 6. reduction
 // ---------------------------------------------------------------------------

@@ -107,6 +107,10 @@ __global__ void accumulate_kernel(const uint32_t *__restrict__ keys, const uint3
 __global__ void merge_heads_kernel(const uint32_t *__restrict__ hb_in, const xyzz *__restrict__ hp_in, unsigned n_in, unsigned chunk,
                                    xyzz *__restrict__ buckets, uint32_t *__restrict__ hb_out, xyzz *__restrict__ hp_out);
 
+// buckets += chunk_buckets for every slot flagged in chunk_flags
+__global__ void merge_chunk_buckets_kernel(xyzz *__restrict__ buckets, uint8_t *__restrict__ flags, const xyzz *__restrict__ chunk_buckets,
+                                           const uint8_t *__restrict__ chunk_flags, unsigned slots);
+
 // ---------------------------------------------------------------------------
 // 6. reduction
 // ---------------------------------------------------------------------------

@@ -210,6 +210,56 @@ def test_events_and_callbacks(gpu, oracle):
     bc.free(bd)
 
 
+@pytest.mark.parametrize("log_n,smem,bases_on_host", [(19, "pinned", False), (20, "pageable", False), (21, "pinned", True),
+                                                     (22, "pinned", False)])
+def test_chunked_host_inputs(gpu, oracle, log_n, smem, bases_on_host):
+    """Host-resident inputs of 2^19 points and more are processed in 2-3 chunks whose
+    copies overlap the previous chunk's work; every chunk after the first is folded
+    into the MSM's buckets.  Skewed scalars put the heavy buckets in every chunk."""
+    n = 1 << log_n
+    scalars, k = synth.workload("skewed" if log_n % 2 else "uniform", n, 200 + log_n)
+    bd, bases = generated_bases(gpu, k)
+    if bases_on_host:  # pageable bases and pinned scalars, both copied chunk by chunk
+        bc = gpu.bc
+        bc.free(bd)
+        hs, hs_ptr = bc.pinned_array(scalars.shape)
+        hs[...] = scalars
+        res = np.zeros((254, 24), np.uint32)
+        bc.msm(gpu.pool, gpu.stream, np.ascontiguousarray(bases), hs_ptr, res, log_n)
+        bc.stream_synchronize(gpu.stream)
+        bc.free_host(hs_ptr)
+    else:
+        res = gpu.msm(None, scalars, scalars_mem=smem, bases_dev=bd)
+        gpu.bc.free(bd)
+    assert oracle.horner(res) == oracle.msm_checksum(k, scalars)
+
+
+def test_chunked_events_and_callbacks(gpu, oracle):
+    """The h2d event and callback fire after the last chunk's copy, d2h after the results."""
+    import bellman_cuda as bcm
+    bc = gpu.bc
+    n = 1 << 20
+    scalars, k = synth.workload("uniform", n, 211)
+    bd, _ = generated_bases(gpu, k)
+    hs, hs_ptr = bc.pinned_array(scalars.shape)
+    hs[...] = scalars
+    fired = []
+    cb = bcm.HOST_FN(lambda data: fired.append(data))
+    e1, e2 = bc.event_create(), bc.event_create()
+    res = np.zeros((254, 24), np.uint32)
+    bc.msm(gpu.pool, gpu.stream, bd, hs_ptr, res, 20, h2d_event=e1, h2d_callback=cb, h2d_data=1,
+           d2h_event=e2, d2h_callback=cb, d2h_data=2)
+    bc.stream_synchronize(gpu.stream)
+    bc.event_synchronize(e1)
+    bc.event_synchronize(e2)
+    assert sorted(fired) == [1, 2]
+    assert oracle.horner(res) == oracle.msm_checksum(k, scalars)
+    for ev in (e1, e2):
+        bc.event_destroy(ev)
+    bc.free(bd)
+    bc.free_host(hs_ptr)
+
+
 def test_invalid_arguments(gpu):
     bc = gpu.bc
     res = np.zeros((254, 24), np.uint32)
