@@ -177,6 +177,14 @@ class BellmanCuda:
                                                   ctypes.POINTER(ctypes.c_uint)],
                 "msm_b200_measure_mul_throughput": [u, ctypes.POINTER(ctypes.c_double)],
                 "msm_b200_execute_no_alloc_async": [Handle, vp, vp, vp, u],
+                "msm_b200_base_table_create": [ctypes.POINTER(vp), vp, u, ctypes.POINTER(u), u, Handle],
+                "msm_b200_base_table_bytes": [vp, ctypes.POINTER(sz)],
+                "msm_b200_base_table_destroy": [vp],
+                "msm_b200_batch_window_bits": [u, ctypes.POINTER(u)],
+                "msm_b200_batch_create": [ctypes.POINTER(vp), vp, ctypes.POINTER(u), u, ctypes.POINTER(u)],
+                "msm_b200_batch_execute_async": [vp, ctypes.POINTER(vp), ctypes.POINTER(vp), Handle],
+                "msm_b200_batch_info": [vp, ctypes.POINTER(sz), ctypes.POINTER(u), ctypes.POINTER(ctypes.c_ulonglong)],
+                "msm_b200_batch_destroy": [vp],
             }
             for name, args in ext.items():
                 f = getattr(L, name)
@@ -365,6 +373,56 @@ class BellmanCuda:
     def msm_no_alloc(self, stream: Handle, bases, scalars, results, count: int) -> int:
         """msm_b200_execute_no_alloc_async: device buffers only, count <= NO_ALLOC_MAX_COUNT; returns the bc_error."""
         return self.lib.msm_b200_execute_no_alloc_async(stream, _ptr(bases), _ptr(scalars), _ptr(results), count)
+
+    # -- batched MSMs over a resident base table -------------------------------
+    def base_table_create(self, bases, count: int, stream: Handle, window_bits=None) -> int:
+        """Resident table (+ precomputed window multiples) over `count` bases; returns its handle."""
+        h = ctypes.c_void_p()
+        widths = list(window_bits or [])
+        arr = (ctypes.c_uint * max(1, len(widths)))(*widths)
+        self.check(self.lib.msm_b200_base_table_create(ctypes.byref(h), _ptr(bases), count, arr if widths else None, len(widths), stream),
+                   "msm_b200_base_table_create")
+        return h.value
+
+    def base_table_bytes(self, table: int) -> int:
+        b = ctypes.c_size_t()
+        self.check(self.lib.msm_b200_base_table_bytes(table, ctypes.byref(b)), "msm_b200_base_table_bytes")
+        return b.value
+
+    def base_table_destroy(self, table: int) -> None:
+        self.check(self.lib.msm_b200_base_table_destroy(table), "msm_b200_base_table_destroy")
+
+    def batch_window_bits(self, count: int) -> int:
+        c = ctypes.c_uint()
+        self.check(self.lib.msm_b200_batch_window_bits(count, ctypes.byref(c)), "msm_b200_batch_window_bits")
+        return c.value
+
+    def batch_create_raw(self, table: int, counts, window_bits=None):
+        """(bc_error, handle) of msm_b200_batch_create."""
+        h = ctypes.c_void_p()
+        cnt = (ctypes.c_uint * len(counts))(*[int(c) for c in counts])
+        wb = (ctypes.c_uint * len(counts))(*[int(c) for c in window_bits]) if window_bits is not None else None
+        rc = self.lib.msm_b200_batch_create(ctypes.byref(h), table, cnt, len(counts), wb)
+        return rc, h.value
+
+    def batch_create(self, table: int, counts, window_bits=None) -> int:
+        rc, h = self.batch_create_raw(table, counts, window_bits)
+        self.check(rc, "msm_b200_batch_create")
+        return h
+
+    def batch_execute(self, batch: int, scalars, results, stream: Handle) -> None:
+        sp = (ctypes.c_void_p * len(scalars))(*[_ptr(x) for x in scalars])
+        rp = (ctypes.c_void_p * len(results))(*[_ptr(x) for x in results])
+        self.check(self.lib.msm_b200_batch_execute_async(batch, sp, rp, stream), "msm_b200_batch_execute_async")
+
+    def batch_info(self, batch: int):
+        """(scratch bytes, kernels per execution, (window, point) entries)."""
+        b, k, e = ctypes.c_size_t(), ctypes.c_uint(), ctypes.c_ulonglong()
+        self.check(self.lib.msm_b200_batch_info(batch, ctypes.byref(b), ctypes.byref(k), ctypes.byref(e)), "msm_b200_batch_info")
+        return b.value, k.value, e.value
+
+    def batch_destroy(self, batch: int) -> None:
+        self.check(self.lib.msm_b200_batch_destroy(batch), "msm_b200_batch_destroy")
 
     def default_window_bits(self, count: int) -> int:
         c = ctypes.c_uint()

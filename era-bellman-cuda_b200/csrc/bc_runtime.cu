@@ -146,13 +146,6 @@ using namespace bn254;
 constexpr unsigned COMB_DIGITS = 64, COMB_VALUES = 15;
 __device__ affine g_comb_table[COMB_DIGITS * COMB_VALUES];
 
-__device__ __forceinline__ affine xyzz_to_affine(const xyzz &p) {
-  const fe inv = fq::inverse(fq::mul(p.zz, p.zzz)); // 1 / (ZZ ZZZ)
-  affine a;
-  a.x = fq::reduce_full(fq::mul(p.x, fq::mul(p.zzz, inv)));
-  a.y = fq::reduce_full(fq::mul(p.y, fq::mul(p.zz, inv)));
-  return a;
-}
 
 __global__ void comb_table_kernel() {
   const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -171,7 +164,7 @@ __global__ void comb_table_kernel() {
   xyzz acc = base;
   for (unsigned k = 1; k < v; k++)
     acc = curve::add(acc, base);
-  g_comb_table[t] = xyzz_to_affine(acc);
+  g_comb_table[t] = curve::to_affine(acc);
 }
 
 __global__ void generator_multiples_kernel(const fe *__restrict__ k, affine *__restrict__ out, unsigned count) {
@@ -190,7 +183,7 @@ __global__ void generator_multiples_kernel(const fe *__restrict__ k, affine *__r
     out[i].y = fq::zero();
     return;
   }
-  out[i] = xyzz_to_affine(acc);
+  out[i] = curve::to_affine(acc);
 }
 
 std::mutex comb_lock;

@@ -174,6 +174,16 @@ struct curve {
     return r;
   }
 
+  // XYZZ -> affine for a finite p: one inversion of ZZ ZZZ gives both
+  // 1/ZZ = ZZZ / (ZZ ZZZ) and 1/ZZZ = ZZ / (ZZ ZZZ).  Output fully reduced.
+  static BN_HD_COLD affine to_affine(const xyzz &p) {
+    const fe inv = fq::inverse(fq::mul(p.zz, p.zzz));
+    affine a;
+    a.x = fq::reduce_full(fq::mul(p.x, fq::mul(p.zzz, inv)));
+    a.y = fq::reduce_full(fq::mul(p.y, fq::mul(p.zz, inv)));
+    return a;
+  }
+
   // XYZZ -> Jacobian (x = X/Z^2, y = Y/Z^3) with Z = ZZZ: since ZZ^3 = ZZZ^2,
   // X_J = X ZZ^2 and Y_J = Y ZZZ^2.  Output fully reduced; infinity is
   // (0, 1, 0) in Montgomery form, the reference's encoding (src/ec.cuh:139).

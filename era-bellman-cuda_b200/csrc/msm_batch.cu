@@ -1,0 +1,719 @@
+// Batched MSM over one resident base table (no counterpart in the reference).
+//
+// A base table holds N affine points on the device and, for every window
+// width c it is built for, the precomputed multiples
+//     M_c[j][i] = 2^(c j) * P_i,   j < W(c) = ceil(254 / c),
+// so that an MSM over a prefix of the table needs ONE set of 2^(c-1) buckets
+// instead of W(c): the digit of window j of scalar i selects M_c[j][i].
+//
+// A batch is a fixed list of instance sizes n_k (any lengths, prefixes of the
+// table).  All instances run as one kernel chain:
+//   digits       every point of every instance, W(c_k) signed digits each, into
+//                its instance's segment of W(c_k) * n_k (key, value) entries
+//   sort         segmented LSD radix sort, tile list over all segments
+//   zero counts  per segment
+//   accumulate   the nonzero entries of all segments split into equal ranges,
+//                one per thread: the (instance, bucket-range) work list
+//   merge heads  as in the plain pipeline
+//   reduction    per group of instances with the same c (one "window" each),
+//                the plain pipeline's reduction kernels on the group's buckets,
+//                then a gather into each instance's 254 results
+// The chain is captured once in a CUDA graph; every execution only writes the
+// instances' scalar and result pointers and replays the graph.
+#include "batch_tuning.h"
+#include "bellman-cuda-b200.h"
+#include "msm_device.cuh"
+#include "msm_host.cuh"
+
+#include <algorithm>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <vector>
+
+namespace msm_b200 {
+
+#define CHECK(statement)                                                                                                                       \
+  do {                                                                                                                                         \
+    cudaError_t check_result_ = (statement);                                                                                                   \
+    if (check_result_ != cudaSuccess)                                                                                                          \
+      return check_result_;                                                                                                                    \
+  } while (0)
+
+constexpr unsigned MAX_BATCH = MSM_B200_MAX_BATCH;
+constexpr unsigned MAX_TABLE_BITS = 24;
+constexpr unsigned IO_CHUNK = 64; // instances per descriptor-update launch
+
+static unsigned ceil_log2_u(unsigned long long v) {
+  unsigned r = 0;
+  while ((1ull << r) < v)
+    r++;
+  return r;
+}
+
+static unsigned windows_for(unsigned c) { return (RESULT_BITS + c - 1) / c; }
+
+unsigned batch_window_bits(unsigned n) {
+  const unsigned lg = ceil_log2_u(n);
+  for (const batch_tuning_row &row : BATCH_TUNING)
+    if (lg <= row.max_log_n)
+      return row.window_bits;
+  return BATCH_TUNING[sizeof(BATCH_TUNING) / sizeof(BATCH_TUNING[0]) - 1].window_bits;
+}
+
+// ---------------------------------------------------------------------------
+// device descriptors
+// ---------------------------------------------------------------------------
+struct batch_instance {
+  unsigned long long entry_offset; // first entry of the instance's segment
+  const affine *table;             // M_c: table[j * stride + i] = 2^(c j) P_i
+  unsigned n, c, windows, stride;
+  unsigned entries;     // windows * n
+  unsigned tiles;       // sort tiles of the segment
+  unsigned tile_base;   // first global sort tile of the segment
+  unsigned bucket_base; // first bucket slot (slot 0 holds |d| = 2^(c-1))
+};
+
+struct batch_io {
+  const fe *scalars; // n Montgomery-form scalars (device)
+  jacobian *results; // 254 Jacobian points (device)
+};
+
+struct batch_io_update {
+  batch_io io[IO_CHUNK];
+  unsigned first, count;
+};
+
+__global__ void batch_set_io_kernel(batch_io *__restrict__ dst, batch_io_update u) {
+  const unsigned k = threadIdx.x;
+  if (k < u.count)
+    dst[u.first + k] = u.io[k];
+}
+
+// 2^c * prev[i] for the points of one window multiple (one thread per point).
+__global__ void __launch_bounds__(128) window_multiples_kernel(const affine *__restrict__ prev, affine *__restrict__ next, unsigned count,
+                                                               unsigned c) {
+  const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count)
+    return;
+  const affine a = prev[i];
+  xyzz p = curve::dbl_affine(a);
+  for (unsigned k = 1; k < c; k++)
+    p = curve::dbl(p);
+  next[i] = curve::to_affine(p); // 2^(cj) P is never infinity: the group order r is an odd prime
+}
+
+// One thread per point of the batch (instances concatenated).
+__global__ void __launch_bounds__(256) batch_digits_kernel(const batch_instance *__restrict__ inst, const unsigned *__restrict__ point_offset,
+                                                           unsigned instances, unsigned total_points, const batch_io *__restrict__ io,
+                                                           uint32_t *__restrict__ keys, uint32_t *__restrict__ vals) {
+  __shared__ unsigned s_off[MAX_BATCH + 1];
+  for (unsigned k = threadIdx.x; k <= instances; k += blockDim.x)
+    s_off[k] = point_offset[k];
+  __syncthreads();
+  const unsigned g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= total_points)
+    return;
+  unsigned lo = 0, hi = instances; // largest k with s_off[k] <= g
+  while (hi - lo > 1) {
+    const unsigned mid = (lo + hi) >> 1;
+    if (s_off[mid] <= g)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  const unsigned k = lo, i = g - s_off[k];
+  const batch_instance d = inst[k];
+  const fe *scalars = io[k].scalars;
+  scalar_digits(load_fe_streaming(scalars + i), d.c, d.windows, [&](unsigned w, uint32_t key, uint32_t negative) {
+    const size_t out = d.entry_offset + (size_t)w * d.n + i;
+    keys[out] = key;
+    vals[out] = (w * d.stride + i) | (negative << 31);
+  });
+}
+
+__global__ void __launch_bounds__(SORT_THREADS) batch_sort_histogram_kernel(const uint32_t *__restrict__ keys, const batch_instance *__restrict__ inst,
+                                                                            const unsigned *__restrict__ tile_seg, unsigned shift,
+                                                                            uint32_t *__restrict__ counts) {
+  const unsigned t = blockIdx.x;
+  const batch_instance d = inst[tile_seg[t]];
+  const unsigned local = t - d.tile_base, base = local * SORT_TILE;
+  sort_histogram_tile(keys + d.entry_offset, base, min(SORT_TILE, d.entries - base), shift, counts + (size_t)d.tile_base * SORT_RADIX + local,
+                      d.tiles);
+}
+
+// one warp per (segment, digit) row
+__global__ void __launch_bounds__(256) batch_sort_scan_kernel(uint32_t *counts, const batch_instance *__restrict__ inst, unsigned rows,
+                                                              uint32_t *__restrict__ totals) {
+  const unsigned row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (row >= rows)
+    return;
+  const batch_instance d = inst[row / SORT_RADIX];
+  sort_scan_row(counts + (size_t)d.tile_base * SORT_RADIX + (size_t)(row % SORT_RADIX) * d.tiles, d.tiles, totals + row);
+}
+
+template <bool STABLE>
+__global__ void __launch_bounds__(SORT_THREADS) batch_sort_scatter_kernel(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
+                                                                          uint32_t *__restrict__ keys_out, uint32_t *__restrict__ vals_out,
+                                                                          const batch_instance *__restrict__ inst,
+                                                                          const unsigned *__restrict__ tile_seg, unsigned shift,
+                                                                          const uint32_t *__restrict__ counts, const uint32_t *__restrict__ totals) {
+  const unsigned t = blockIdx.x;
+  const unsigned k = tile_seg[t];
+  const batch_instance d = inst[k];
+  const unsigned local = t - d.tile_base, base = local * SORT_TILE;
+  sort_scatter_tile<STABLE>(keys_in, vals_in, keys_out, vals_out, d.entry_offset, base, min(SORT_TILE, d.entries - base), shift,
+                            counts + (size_t)d.tile_base * SORT_RADIX + local, d.tiles, totals + (size_t)k * SORT_RADIX);
+}
+
+__global__ void batch_zero_counts_kernel(const uint32_t *__restrict__ keys, const batch_instance *__restrict__ inst, unsigned instances,
+                                         uint32_t *__restrict__ zeros) {
+  const unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= instances)
+    return;
+  const batch_instance d = inst[k];
+  const uint32_t *seg = keys + d.entry_offset;
+  unsigned lo = 0, hi = d.entries; // first index with key != 0
+  while (lo < hi) {
+    const unsigned mid = (lo + hi) >> 1;
+    if (seg[mid] == 0)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  zeros[k] = lo;
+}
+
+// The batch's segments for accumulate_ranges: one per instance.
+struct table_segments {
+  const unsigned long long *s_first, *s_end, *s_prefix;
+  const uint32_t *s_bucket, *s_mask;
+  const affine *const *s_table;
+  unsigned segments;
+  __device__ __forceinline__ unsigned count() const { return segments; }
+  __device__ __forceinline__ unsigned long long prefix(unsigned s) const { return s_prefix[s]; }
+  __device__ __forceinline__ size_t first(unsigned s) const { return s_first[s]; }
+  __device__ __forceinline__ size_t end(unsigned s) const { return s_end[s]; }
+  __device__ __forceinline__ bool empty(unsigned s) const { return s_first[s] == s_end[s]; }
+  __device__ __forceinline__ unsigned bucket(unsigned s, uint32_t key) const { return s_bucket[s] + (key & s_mask[s]); }
+  __device__ __forceinline__ const affine *base(unsigned s, uint32_t val) const { return s_table[s] + (val & 0x7fffffffu); }
+};
+
+__global__ void __launch_bounds__(ACC_THREADS, ACC_MIN_BLOCKS) batch_accumulate_kernel(
+    const uint32_t *__restrict__ keys, const uint32_t *__restrict__ vals, const batch_instance *__restrict__ inst, unsigned instances,
+    const uint32_t *__restrict__ zeros, unsigned total_threads, xyzz *__restrict__ buckets, uint8_t *__restrict__ flags,
+    uint32_t *__restrict__ head_bucket, xyzz *__restrict__ head_point) {
+  __shared__ unsigned long long s_first[MAX_BATCH], s_end[MAX_BATCH], s_prefix[MAX_BATCH + 1];
+  __shared__ uint32_t s_bucket[MAX_BATCH], s_mask[MAX_BATCH];
+  __shared__ const affine *s_table[MAX_BATCH];
+  __shared__ uint4 s_base[2][4][ACC_THREADS];
+  for (unsigned k = threadIdx.x; k < instances; k += blockDim.x) {
+    const batch_instance d = inst[k];
+    s_first[k] = d.entry_offset + zeros[k];
+    s_end[k] = d.entry_offset + d.entries;
+    s_bucket[k] = d.bucket_base;
+    s_mask[k] = (1u << (d.c - 1)) - 1;
+    s_table[k] = d.table;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long acc = 0;
+    for (unsigned k = 0; k < instances; k++) {
+      s_prefix[k] = acc;
+      acc += s_end[k] - s_first[k];
+    }
+    s_prefix[instances] = acc;
+  }
+  __syncthreads();
+  const table_segments seg{s_first, s_end, s_prefix, s_bucket, s_mask, s_table, instances};
+  accumulate_ranges(seg, keys, vals, total_threads, buckets, flags, head_bucket, head_point, s_base);
+}
+
+// Results of the instances of one reduction group (all of window width c):
+// instance members[w] is window w of the group's reduction.  Bit i < c comes
+// from the group's streams exactly as gather_results_kernel places window 0
+// of a plain MSM; bits >= c are infinity.
+__global__ void batch_gather_kernel(const xyzz *__restrict__ streams, const xyzz *__restrict__ buckets, const uint8_t *__restrict__ flags,
+                                    const unsigned *__restrict__ members, unsigned windows, unsigned c, unsigned log_m, unsigned log_g,
+                                    const batch_io *__restrict__ io) {
+  const unsigned gid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= windows * RESULT_BITS)
+    return;
+  const unsigned w = gid / RESULT_BITS, i = gid % RESULT_BITS;
+  xyzz p = curve::infinity();
+  if (i < c) {
+    const size_t base = (size_t)w * stream_stride(log_g);
+    if (i == 0) {
+      p = load_xyzz(streams + base);
+    } else if (i == c - 1) {
+      const size_t slot0 = (size_t)w << (c - 1);
+      if (flags[slot0])
+        p = load_xyzz(buckets + slot0);
+    } else if (i >= log_m && i - log_m < log_g) {
+      p = load_xyzz(streams + base + stream_offset(log_g, i - log_m + 1));
+    }
+  }
+  store_jacobian(io[members[w]].results + i, curve::to_jacobian(p));
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+struct base_table_impl {
+  int device = 0;
+  unsigned count = 0;
+  affine *mult[MAX_TABLE_BITS + 1] = {}; // mult[c]: windows_for(c) * prefix[c] points, or null
+  unsigned prefix[MAX_TABLE_BITS + 1] = {};
+  size_t bytes = 0;
+  ~base_table_impl() {
+    for (affine *m : mult)
+      if (m)
+        cudaFree(m);
+  }
+};
+
+// Builds M_c for the first `prefix` points of `bases` (device memory).
+static cudaError_t build_multiples(base_table_impl &t, unsigned c, unsigned prefix, const affine *bases, cudaStream_t stream) {
+  const unsigned W = windows_for(c);
+  affine *m = nullptr;
+  const size_t bytes = (size_t)W * prefix * sizeof(affine);
+  CHECK(cudaMalloc(&m, bytes));
+  t.mult[c] = m;
+  t.prefix[c] = prefix;
+  t.bytes += bytes;
+  CHECK(cudaMemcpyAsync(m, bases, (size_t)prefix * sizeof(affine), cudaMemcpyDeviceToDevice, stream));
+  for (unsigned j = 1; j < W; j++) {
+    window_multiples_kernel<<<(prefix + 127) / 128, 128, 0, stream>>>(m + (size_t)(j - 1) * prefix, m + (size_t)j * prefix, prefix, c);
+    CHECK(cudaGetLastError());
+  }
+  return cudaSuccess;
+}
+
+cudaError_t base_table_create(base_table_impl **out, const void *bases, unsigned count, const unsigned *window_bits, unsigned widths,
+                              cudaStream_t stream) {
+  if (!out || !bases || count == 0 || (reinterpret_cast<uintptr_t>(bases) & 15))
+    return cudaErrorInvalidValue;
+  // window widths and, per width, the longest prefix an instance of that width can use
+  std::map<unsigned, unsigned> want;
+  if (widths) {
+    for (unsigned k = 0; k < widths; k++) {
+      if (window_bits[k] < 2 || window_bits[k] > MAX_TABLE_BITS)
+        return cudaErrorInvalidValue;
+      want[window_bits[k]] = count;
+    }
+  } else {
+    for (unsigned lg = 0; (1ull << lg) < 2ull * count && lg <= 31; lg++) {
+      const unsigned n = (unsigned)std::min<unsigned long long>(count, 1ull << lg);
+      unsigned &p = want[batch_window_bits(n)];
+      p = std::max(p, n);
+    }
+  }
+  base_table_impl *t = new (std::nothrow) base_table_impl;
+  if (!t)
+    return cudaErrorMemoryAllocation;
+  cudaError_t status = cudaGetDevice(&t->device);
+  t->count = count;
+  affine *staged = nullptr;
+  cudaPointerAttributes attr{};
+  if (status == cudaSuccess)
+    status = cudaPointerGetAttributes(&attr, bases);
+  const bool host = attr.type == cudaMemoryTypeUnregistered || attr.type == cudaMemoryTypeHost;
+  const affine *src = static_cast<const affine *>(bases);
+  if (status == cudaSuccess && host) {
+    status = cudaMalloc(&staged, (size_t)count * sizeof(affine));
+    if (status == cudaSuccess)
+      status = cudaMemcpyAsync(staged, bases, (size_t)count * sizeof(affine), cudaMemcpyHostToDevice, stream);
+    src = staged;
+  }
+  for (auto it = want.begin(); status == cudaSuccess && it != want.end(); ++it)
+    status = build_multiples(*t, it->first, it->second, src, stream);
+  if (status == cudaSuccess)
+    status = cudaStreamSynchronize(stream);
+  if (staged)
+    cudaFree(staged);
+  if (status != cudaSuccess) {
+    delete t;
+    return status;
+  }
+  *out = t;
+  return cudaSuccess;
+}
+
+struct batch_group {
+  unsigned c;
+  std::vector<unsigned> members; // instances, in bucket order
+  plan p;                        // reduction geometry (windows = members)
+  unsigned bucket_base;
+  size_t tree[2], streams[2], members_dev;
+};
+
+struct batch_impl {
+  int device = 0;
+  const base_table_impl *table = nullptr;
+  unsigned instances = 0;
+  unsigned long long total_entries = 0;
+  unsigned total_points = 0, total_tiles = 0, slots = 0, sort_passes = 0, acc_threads = 0;
+  std::vector<batch_instance> inst;
+  std::vector<batch_group> groups;
+  uint8_t *scratch = nullptr;
+  size_t scratch_bytes = 0;
+  size_t keys[2], vals[2], counts, totals, zeros, buckets, flags, hb[2], hp[2], inst_dev, point_offset, tile_seg, io;
+  cudaStream_t capture = nullptr;
+  std::vector<cudaStream_t> forks;
+  std::vector<cudaEvent_t> fork_events;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  unsigned launches = 0;
+  ~batch_impl() {
+    if (exec)
+      cudaGraphExecDestroy(exec);
+    if (graph)
+      cudaGraphDestroy(graph);
+    for (cudaEvent_t e : fork_events)
+      cudaEventDestroy(e);
+    for (cudaStream_t s : forks)
+      cudaStreamDestroy(s);
+    if (capture)
+      cudaStreamDestroy(capture);
+    if (scratch)
+      cudaFree(scratch);
+  }
+  template <class T> T *at(size_t off) const { return reinterpret_cast<T *>(scratch + off); }
+};
+
+static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
+
+// Enqueues the whole chain on b.capture (and its forks for the reductions).
+static cudaError_t enqueue_batch(batch_impl &b) {
+  cudaStream_t s = b.capture;
+  unsigned launched = 0;
+  uint32_t *keys[2] = {b.at<uint32_t>(b.keys[0]), b.at<uint32_t>(b.keys[1])};
+  uint32_t *vals[2] = {b.at<uint32_t>(b.vals[0]), b.at<uint32_t>(b.vals[1])};
+  const batch_instance *inst = b.at<batch_instance>(b.inst_dev);
+  const batch_io *io = b.at<batch_io>(b.io);
+  uint32_t *counts = b.at<uint32_t>(b.counts), *totals = b.at<uint32_t>(b.totals), *zeros = b.at<uint32_t>(b.zeros);
+  const unsigned *tile_seg = b.at<unsigned>(b.tile_seg);
+  xyzz *buckets = b.at<xyzz>(b.buckets);
+  uint8_t *flags = b.at<uint8_t>(b.flags);
+  uint32_t *hb[2] = {b.at<uint32_t>(b.hb[0]), b.at<uint32_t>(b.hb[1])};
+  xyzz *hp[2] = {b.at<xyzz>(b.hp[0]), b.at<xyzz>(b.hp[1])};
+
+  CHECK(cudaMemsetAsync(flags, 0, b.slots, s));
+  batch_digits_kernel<<<(b.total_points + 255) / 256, 256, 0, s>>>(inst, b.at<unsigned>(b.point_offset), b.instances, b.total_points, io, keys[0],
+                                                                   vals[0]);
+  CHECK(cudaGetLastError());
+  launched++;
+  int cur = 0;
+  const unsigned rows = b.instances * SORT_RADIX;
+  for (unsigned pass = 0; pass < b.sort_passes; pass++) {
+    const unsigned shift = pass * SORT_RADIX_BITS;
+    batch_sort_histogram_kernel<<<b.total_tiles, SORT_THREADS, 0, s>>>(keys[cur], inst, tile_seg, shift, counts);
+    CHECK(cudaGetLastError());
+    batch_sort_scan_kernel<<<(rows * 32 + 255) / 256, 256, 0, s>>>(counts, inst, rows, totals);
+    CHECK(cudaGetLastError());
+    if (pass == 0)
+      batch_sort_scatter_kernel<false><<<b.total_tiles, SORT_THREADS, 0, s>>>(keys[cur], vals[cur], keys[cur ^ 1], vals[cur ^ 1], inst, tile_seg,
+                                                                             shift, counts, totals);
+    else
+      batch_sort_scatter_kernel<true><<<b.total_tiles, SORT_THREADS, 0, s>>>(keys[cur], vals[cur], keys[cur ^ 1], vals[cur ^ 1], inst, tile_seg,
+                                                                            shift, counts, totals);
+    CHECK(cudaGetLastError());
+    launched += 3;
+    cur ^= 1;
+  }
+  batch_zero_counts_kernel<<<(b.instances + 127) / 128, 128, 0, s>>>(keys[cur], inst, b.instances, zeros);
+  CHECK(cudaGetLastError());
+  batch_accumulate_kernel<<<(b.acc_threads + ACC_THREADS - 1) / ACC_THREADS, ACC_THREADS, 0, s>>>(
+      keys[cur], vals[cur], inst, b.instances, zeros, b.acc_threads, buckets, flags, hb[0], hp[0]);
+  CHECK(cudaGetLastError());
+  launched += 2;
+  unsigned heads = b.acc_threads;
+  int h = 0;
+  while (heads > 1) {
+    const unsigned out = (heads + 3) / 4;
+    merge_heads_kernel<<<(out + ACC_THREADS - 1) / ACC_THREADS, ACC_THREADS, 0, s>>>(hb[h], hp[h], heads, 4, buckets, hb[h ^ 1], hp[h ^ 1]);
+    CHECK(cudaGetLastError());
+    launched++;
+    heads = out;
+    h ^= 1;
+  }
+  // reductions: one chain per window width, each on its own forked stream
+  CHECK(cudaEventRecord(b.fork_events[0], s));
+  for (size_t g = 0; g < b.groups.size(); g++) {
+    const batch_group &grp = b.groups[g];
+    const plan &p = grp.p;
+    cudaStream_t fs = b.forks[g];
+    CHECK(cudaStreamWaitEvent(fs, b.fork_events[0], 0));
+    xyzz *gb = buckets + grp.bucket_base;
+    const uint8_t *gf = flags + grp.bucket_base;
+    xyzz *tree[2] = {b.at<xyzz>(grp.tree[0]), b.at<xyzz>(grp.tree[1])};
+    xyzz *streams[2] = {b.at<xyzz>(grp.streams[0]), b.at<xyzz>(grp.streams[1])};
+    const unsigned group_threads = p.windows << p.log_g;
+    reduce_groups_kernel<<<(group_threads + ACC_THREADS - 1) / ACC_THREADS, ACC_THREADS, 0, fs>>>(gb, gf, p.windows, p.log_b, p.log_m, tree[0],
+                                                                                                   streams[0]);
+    CHECK(cudaGetLastError());
+    launched++;
+    int t = 0;
+    for (unsigned level = 0; level < p.log_g; level++) {
+      const unsigned threads = p.windows * ((1u << p.log_g) >> (level + 1));
+      reduce_tree_kernel<<<(threads + ACC_THREADS - 1) / ACC_THREADS, ACC_THREADS, 0, fs>>>(tree[t], tree[t ^ 1], streams[0], p.windows, p.log_g,
+                                                                                             level);
+      CHECK(cudaGetLastError());
+      launched++;
+      t ^= 1;
+    }
+    int si = 0;
+    unsigned divisor = 1;
+    while (divisor < p.groups) {
+      const unsigned len_out = ((p.groups + divisor - 1) / divisor + p.sum_fanin - 1) / p.sum_fanin;
+      const dim3 grid((len_out + ACC_THREADS - 1) / ACC_THREADS, p.windows * (p.log_g + 1));
+      reduce_streams_kernel<<<grid, ACC_THREADS, 0, fs>>>(streams[si], streams[si ^ 1], p.windows, p.log_g, p.sum_fanin, divisor);
+      CHECK(cudaGetLastError());
+      launched++;
+      divisor *= p.sum_fanin;
+      si ^= 1;
+    }
+    const unsigned gather_threads = p.windows * RESULT_BITS;
+    batch_gather_kernel<<<(gather_threads + 127) / 128, 128, 0, fs>>>(streams[si], gb, gf, b.at<unsigned>(grp.members_dev), p.windows, p.c,
+                                                                      p.log_m, p.log_g, io);
+    CHECK(cudaGetLastError());
+    launched++;
+    CHECK(cudaEventRecord(b.fork_events[g + 1], fs));
+    CHECK(cudaStreamWaitEvent(s, b.fork_events[g + 1], 0));
+  }
+  b.launches = launched;
+  return cudaSuccess;
+}
+
+cudaError_t batch_create(batch_impl **out, const base_table_impl *table, const unsigned *counts, unsigned instances, const unsigned *window_bits) {
+  if (!out || !table || !counts || instances == 0 || instances > MAX_BATCH)
+    return cudaErrorInvalidValue;
+  int device = 0;
+  CHECK(cudaGetDevice(&device));
+  if (device != table->device)
+    return cudaErrorInvalidDevice;
+  int sms = 0;
+  CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  batch_impl *bp = new (std::nothrow) batch_impl;
+  if (!bp)
+    return cudaErrorMemoryAllocation;
+  std::unique_ptr<batch_impl> owner(bp);
+  batch_impl &b = *bp;
+  b.device = device;
+  b.table = table;
+  b.instances = instances;
+  b.inst.resize(instances);
+  // instance geometry; reduction groups by window width (buckets of a group contiguous)
+  std::map<unsigned, std::vector<unsigned>> by_c;
+  unsigned max_c = 0;
+  std::vector<unsigned> point_offset(instances + 1, 0);
+  unsigned long long points = 0;
+  for (unsigned k = 0; k < instances; k++) {
+    const unsigned n = counts[k];
+    const unsigned c = window_bits && window_bits[k] ? window_bits[k] : batch_window_bits(n);
+    if (n == 0 || c < 2 || c > MAX_TABLE_BITS || !table->mult[c] || n > table->prefix[c])
+      return cudaErrorInvalidValue;
+    batch_instance &d = b.inst[k];
+    d.n = n;
+    d.c = c;
+    d.windows = windows_for(c);
+    d.stride = table->prefix[c];
+    d.table = table->mult[c];
+    d.entries = d.windows * n;
+    d.entry_offset = b.total_entries;
+    d.tiles = (d.entries + SORT_TILE - 1) / SORT_TILE;
+    d.tile_base = b.total_tiles;
+    if ((unsigned long long)d.windows * n >= (1ull << 31) || d.windows * (unsigned long long)d.stride >= (1ull << 31))
+      return cudaErrorInvalidValue;
+    b.total_entries += d.entries;
+    b.total_tiles += d.tiles;
+    point_offset[k] = (unsigned)points;
+    points += n;
+    max_c = std::max(max_c, c);
+    by_c[c].push_back(k);
+  }
+  if (points >= (1ull << 32) || b.total_tiles >= (1u << 31))
+    return cudaErrorInvalidValue;
+  point_offset[instances] = (unsigned)points;
+  b.total_points = (unsigned)points;
+  b.sort_passes = (max_c + SORT_RADIX_BITS - 1) / SORT_RADIX_BITS;
+  for (auto &kv : by_c) {
+    batch_group g;
+    g.c = kv.first;
+    g.members = kv.second;
+    g.bucket_base = b.slots;
+    g.p = make_plan(1, g.c, sms);
+    g.p.windows = (unsigned)g.members.size();
+    for (unsigned w = 0; w < g.members.size(); w++)
+      b.inst[g.members[w]].bucket_base = b.slots + (w << (g.c - 1));
+    b.slots += (unsigned)g.members.size() << (g.c - 1);
+    b.groups.push_back(g);
+  }
+  const unsigned long long full = (unsigned long long)sms * ACC_MIN_BLOCKS * ACC_THREADS;
+  b.acc_threads = (unsigned)std::max(1ull, std::min(full, (b.total_entries + 7) / 8));
+  // scratch layout
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    const size_t at = off;
+    off += align256(bytes);
+    return at;
+  };
+  for (int i = 0; i < 2; i++) {
+    b.keys[i] = take(b.total_entries * 4);
+    b.vals[i] = take(b.total_entries * 4);
+  }
+  b.counts = take((size_t)b.total_tiles * SORT_RADIX * 4);
+  b.totals = take((size_t)instances * SORT_RADIX * 4);
+  b.zeros = take((size_t)instances * 4);
+  b.buckets = take((size_t)b.slots * sizeof(xyzz));
+  b.flags = take(b.slots);
+  for (int i = 0; i < 2; i++) {
+    b.hb[i] = take((size_t)b.acc_threads * 4);
+    b.hp[i] = take((size_t)b.acc_threads * sizeof(xyzz));
+  }
+  for (batch_group &g : b.groups) {
+    for (int i = 0; i < 2; i++) {
+      g.tree[i] = take(((size_t)g.p.windows << g.p.log_g) * sizeof(xyzz));
+      g.streams[i] = take((size_t)g.p.windows * stream_stride(g.p.log_g) * sizeof(xyzz));
+    }
+    g.members_dev = take(g.members.size() * 4);
+  }
+  b.inst_dev = take(instances * sizeof(batch_instance));
+  b.point_offset = take((instances + 1) * 4);
+  b.tile_seg = take((size_t)b.total_tiles * 4);
+  b.io = take(instances * sizeof(batch_io));
+  b.scratch_bytes = off;
+  CHECK(cudaMalloc(&b.scratch, b.scratch_bytes));
+  // constant descriptors
+  std::vector<unsigned> tile_seg(b.total_tiles);
+  for (unsigned k = 0; k < instances; k++)
+    std::fill(tile_seg.begin() + b.inst[k].tile_base, tile_seg.begin() + b.inst[k].tile_base + b.inst[k].tiles, k);
+  CHECK(cudaMemcpy(b.scratch + b.inst_dev, b.inst.data(), instances * sizeof(batch_instance), cudaMemcpyHostToDevice));
+  CHECK(cudaMemcpy(b.scratch + b.point_offset, point_offset.data(), (instances + 1) * 4, cudaMemcpyHostToDevice));
+  CHECK(cudaMemcpy(b.scratch + b.tile_seg, tile_seg.data(), tile_seg.size() * 4, cudaMemcpyHostToDevice));
+  for (const batch_group &g : b.groups)
+    CHECK(cudaMemcpy(b.scratch + g.members_dev, g.members.data(), g.members.size() * 4, cudaMemcpyHostToDevice));
+  CHECK(cudaMemset(b.scratch + b.io, 0, instances * sizeof(batch_io)));
+  // capture the chain
+  CHECK(cudaStreamCreateWithFlags(&b.capture, cudaStreamNonBlocking));
+  b.forks.resize(b.groups.size());
+  b.fork_events.resize(b.groups.size() + 1);
+  for (auto &fs : b.forks)
+    CHECK(cudaStreamCreateWithFlags(&fs, cudaStreamNonBlocking));
+  for (auto &e : b.fork_events)
+    CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  CHECK(cudaStreamBeginCapture(b.capture, cudaStreamCaptureModeThreadLocal));
+  const cudaError_t enq = enqueue_batch(b);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t end = cudaStreamEndCapture(b.capture, &graph);
+  b.graph = graph;
+  CHECK(enq);
+  CHECK(end);
+  CHECK(cudaGraphInstantiate(&b.exec, b.graph, 0));
+  *out = owner.release();
+  return cudaSuccess;
+}
+
+cudaError_t batch_execute(batch_impl *b, const void *const *scalars, void *const *results, cudaStream_t stream) {
+  if (!b || !scalars || !results)
+    return cudaErrorInvalidValue;
+  int device = 0;
+  CHECK(cudaGetDevice(&device));
+  if (device != b->device)
+    return cudaErrorInvalidDevice;
+  for (unsigned k = 0; k < b->instances; k++)
+    if (!scalars[k] || !results[k] || (reinterpret_cast<uintptr_t>(scalars[k]) & 15) || (reinterpret_cast<uintptr_t>(results[k]) & 15))
+      return cudaErrorInvalidValue;
+  batch_io *io = b->at<batch_io>(b->io);
+  for (unsigned first = 0; first < b->instances; first += IO_CHUNK) {
+    batch_io_update u{};
+    u.first = first;
+    u.count = std::min(IO_CHUNK, b->instances - first);
+    for (unsigned k = 0; k < u.count; k++) {
+      u.io[k].scalars = static_cast<const fe *>(scalars[first + k]);
+      u.io[k].results = static_cast<jacobian *>(results[first + k]);
+    }
+    batch_set_io_kernel<<<1, IO_CHUNK, 0, stream>>>(io, u);
+    CHECK(cudaGetLastError());
+  }
+  return cudaGraphLaunch(b->exec, stream);
+}
+
+cudaError_t batch_set_up() {
+  CHECK(cudaFuncSetAttribute(batch_accumulate_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 50));
+  return cudaSuccess;
+}
+
+} // namespace msm_b200
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+bc_error msm_b200_base_table_create(msm_b200_base_table *table, const void *bases, unsigned count, const unsigned *window_bits, unsigned widths,
+                                    bc_stream stream) {
+  if (!table)
+    return bc_error_invalid_value;
+  msm_b200::base_table_impl *t = nullptr;
+  const cudaError_t e = msm_b200::base_table_create(&t, bases, count, window_bits, widths, static_cast<cudaStream_t>(stream.handle));
+  *table = reinterpret_cast<msm_b200_base_table>(t);
+  return static_cast<bc_error>(e);
+}
+
+bc_error msm_b200_base_table_bytes(msm_b200_base_table table, size_t *bytes) {
+  if (!table || !bytes)
+    return bc_error_invalid_value;
+  *bytes = reinterpret_cast<msm_b200::base_table_impl *>(table)->bytes;
+  return bc_success;
+}
+
+bc_error msm_b200_base_table_destroy(msm_b200_base_table table) {
+  delete reinterpret_cast<msm_b200::base_table_impl *>(table);
+  return bc_success;
+}
+
+bc_error msm_b200_batch_window_bits(unsigned count, unsigned *window_bits) {
+  if (!window_bits || count == 0)
+    return bc_error_invalid_value;
+  *window_bits = msm_b200::batch_window_bits(count);
+  return bc_success;
+}
+
+bc_error msm_b200_batch_create(msm_b200_batch *batch, msm_b200_base_table table, const unsigned *counts, unsigned instances,
+                               const unsigned *window_bits) {
+  if (!batch)
+    return bc_error_invalid_value;
+  msm_b200::batch_impl *b = nullptr;
+  cudaError_t e = msm_b200::batch_set_up();
+  if (e == cudaSuccess)
+    e = msm_b200::batch_create(&b, reinterpret_cast<const msm_b200::base_table_impl *>(table), counts, instances, window_bits);
+  *batch = reinterpret_cast<msm_b200_batch>(b);
+  return static_cast<bc_error>(e);
+}
+
+bc_error msm_b200_batch_execute_async(msm_b200_batch batch, const void *const *scalars, void *const *results, bc_stream stream) {
+  return static_cast<bc_error>(
+      msm_b200::batch_execute(reinterpret_cast<msm_b200::batch_impl *>(batch), scalars, results, static_cast<cudaStream_t>(stream.handle)));
+}
+
+bc_error msm_b200_batch_info(msm_b200_batch batch, size_t *scratch_bytes, unsigned *kernels, unsigned long long *entries) {
+  if (!batch)
+    return bc_error_invalid_value;
+  const msm_b200::batch_impl *b = reinterpret_cast<const msm_b200::batch_impl *>(batch);
+  if (scratch_bytes)
+    *scratch_bytes = b->scratch_bytes;
+  if (kernels)
+    *kernels = b->launches;
+  if (entries)
+    *entries = b->total_entries;
+  return bc_success;
+}
+
+bc_error msm_b200_batch_destroy(msm_b200_batch batch) {
+  delete reinterpret_cast<msm_b200::batch_impl *>(batch);
+  return bc_success;
+}
+
+} // extern "C"

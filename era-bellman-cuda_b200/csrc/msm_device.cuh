@@ -1,0 +1,470 @@
+// Device helpers shared by the MSM kernels of the plain pipeline
+// (msm_kernels.cu) and of the batched pipeline (msm_batch.cu): 128-bit vector
+// memory access, signed-digit extraction, and the tile-level pieces of the
+// project's LSD radix sort.
+#pragma once
+
+#include "msm_kernels.cuh"
+
+namespace msm_b200 {
+
+// ---------------------------------------------------------------------------
+// 128-bit vector memory helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ fe load_fe_streaming(const fe *p) {
+  const uint4 *q = reinterpret_cast<const uint4 *>(p);
+  const uint4 a = __ldcs(q), b = __ldcs(q + 1);
+  fe r;
+  r.l[0] = a.x, r.l[1] = a.y, r.l[2] = a.z, r.l[3] = a.w;
+  r.l[4] = b.x, r.l[5] = b.y, r.l[6] = b.z, r.l[7] = b.w;
+  return r;
+}
+
+__device__ __forceinline__ affine load_affine(const affine *p) {
+  const uint4 *q = reinterpret_cast<const uint4 *>(p);
+  const uint4 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2), d = __ldg(q + 3);
+  affine r;
+  r.x.l[0] = a.x, r.x.l[1] = a.y, r.x.l[2] = a.z, r.x.l[3] = a.w;
+  r.x.l[4] = b.x, r.x.l[5] = b.y, r.x.l[6] = b.z, r.x.l[7] = b.w;
+  r.y.l[0] = c.x, r.y.l[1] = c.y, r.y.l[2] = c.z, r.y.l[3] = c.w;
+  r.y.l[4] = d.x, r.y.l[5] = d.y, r.y.l[6] = d.z, r.y.l[7] = d.w;
+  return r;
+}
+
+__device__ __forceinline__ xyzz load_xyzz(const xyzz *p) {
+  const uint4 *q = reinterpret_cast<const uint4 *>(p);
+  xyzz r;
+  uint32_t *w = reinterpret_cast<uint32_t *>(&r);
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    const uint4 v = q[i];
+    w[4 * i + 0] = v.x;
+    w[4 * i + 1] = v.y;
+    w[4 * i + 2] = v.z;
+    w[4 * i + 3] = v.w;
+  }
+  return r;
+}
+
+__device__ __forceinline__ void store_xyzz(xyzz *p, const xyzz &v) {
+  uint4 *q = reinterpret_cast<uint4 *>(p);
+  const uint32_t *w = reinterpret_cast<const uint32_t *>(&v);
+#pragma unroll
+  for (int i = 0; i < 8; i++)
+    q[i] = make_uint4(w[4 * i], w[4 * i + 1], w[4 * i + 2], w[4 * i + 3]);
+}
+
+__device__ __forceinline__ void store_jacobian(jacobian *p, const jacobian &v) {
+  uint4 *q = reinterpret_cast<uint4 *>(p);
+  const uint32_t *w = reinterpret_cast<const uint32_t *>(&v);
+#pragma unroll
+  for (int i = 0; i < 6; i++)
+    q[i] = make_uint4(w[4 * i], w[4 * i + 1], w[4 * i + 2], w[4 * i + 3]);
+}
+
+__device__ __forceinline__ uint32_t limb_at(const fe &s, unsigned k) {
+  uint32_t r = 0;
+#pragma unroll
+  for (unsigned j = 0; j < 8; j++)
+    r = (k == j) ? s.l[j] : r;
+  return r;
+}
+
+// ---------------------------------------------------------------------------
+// 1. digits
+// ---------------------------------------------------------------------------
+// Signed windows of one scalar; emit(w, key, negative) for each window.
+template <class EMIT> __device__ __forceinline__ void scalar_digits(const fe &scalar_mont, unsigned c, unsigned windows, EMIT emit) {
+  fe s = fr::from_mont(scalar_mont); // canonical, < r
+  // r - s (s == 0 gives r, which is never the smaller one)
+  const fe m = fr::modulus();
+  fe neg;
+  neg.l[0] = bn254::cc::sub_cc(m.l[0], s.l[0]);
+#pragma unroll
+  for (int k = 1; k < 8; k++)
+    neg.l[k] = bn254::cc::subc_cc(m.l[k], s.l[k]);
+  const bool flip = fr::lt(neg, s);
+  if (flip)
+    s = neg;
+  const uint32_t half = 1u << (c - 1);
+  const uint32_t mask = (1u << c) - 1;
+  uint32_t carry = 0;
+  for (unsigned w = 0; w < windows; w++) {
+    const unsigned bit = w * c;
+    const unsigned limb = bit >> 5;
+    const uint32_t lo = limb < 8 ? limb_at(s, limb) : 0;
+    const uint32_t hi = limb + 1 < 8 ? limb_at(s, limb + 1) : 0;
+    uint32_t raw = (__funnelshift_r(lo, hi, bit & 31) & mask) + carry;
+    uint32_t negative = 0;
+    if (raw > half) {
+      raw = (mask + 1) - raw;
+      negative = 1;
+      carry = 1;
+    } else {
+      carry = 0;
+    }
+    emit(w, raw, negative ^ (flip ? 1u : 0u));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// LSD radix sort, tile level (one 8-bit digit per pass)
+// ---------------------------------------------------------------------------
+constexpr unsigned SORT_WARPS = SORT_THREADS / 32;
+
+__device__ __forceinline__ unsigned sort_digit(uint32_t key, unsigned shift) { return (key >> shift) & (SORT_RADIX - 1); }
+
+// Tile histogram of `count` keys at seg_keys[base..]: out[d * out_stride] =
+// number of keys whose current digit is d.  Per-warp shared counters (no
+// cross-warp contention); the dominant zero digit of sparse scalars is
+// counted with one ballot per warp.
+__device__ __forceinline__ void sort_histogram_tile(const uint32_t *__restrict__ seg_keys, unsigned base, unsigned count, unsigned shift,
+                                                    uint32_t *__restrict__ out, size_t out_stride) {
+  __shared__ uint32_t hist[SORT_WARPS][SORT_RADIX];
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (unsigned d = lane; d < SORT_RADIX; d += 32)
+    hist[warp][d] = 0;
+  __syncwarp();
+#pragma unroll 4
+  for (unsigned k = 0; k < SORT_ITEMS; k++) {
+    const unsigned i = k * SORT_THREADS + threadIdx.x;
+    const bool valid = i < count;
+    const unsigned d = valid ? sort_digit(seg_keys[base + i], shift) : 0;
+    const unsigned zeros = __ballot_sync(0xffffffffu, valid && d == 0);
+    if (valid && d != 0)
+      atomicAdd(&hist[warp][d], 1u);
+    if (lane == 0 && zeros)
+      hist[warp][0] += __popc(zeros);
+  }
+  __syncthreads();
+  for (unsigned d = threadIdx.x; d < SORT_RADIX; d += blockDim.x) {
+    uint32_t sum = 0;
+#pragma unroll
+    for (unsigned k = 0; k < SORT_WARPS; k++)
+      sum += hist[k][d];
+    out[d * out_stride] = sum;
+  }
+}
+
+// One warp: exclusive prefix of row[0..len) in place, the row total into
+// *total.  Lane l scans a contiguous chunk of the row; the chunk sums are
+// scanned across the warp.
+__device__ __forceinline__ void sort_scan_row(uint32_t *r, unsigned len, uint32_t *__restrict__ total) {
+  const unsigned lane = threadIdx.x & 31;
+  const unsigned chunk = (len + 31) / 32;
+  const unsigned beg = min(len, lane * chunk), end = min(len, beg + chunk);
+  uint32_t local = 0;
+  for (unsigned t = beg; t < end; t++)
+    local += r[t];
+  uint32_t incl = local;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const uint32_t u = __shfl_up_sync(0xffffffffu, incl, off);
+    if (lane >= (unsigned)off)
+      incl += u;
+  }
+  uint32_t run = incl - local;
+  for (unsigned t = beg; t < end; t++) {
+    const uint32_t v = r[t];
+    r[t] = run;
+    run += v;
+  }
+  if (lane == 31)
+    *total = incl;
+}
+
+// Exclusive block-wide scan of 256 shared counters by the first 256 threads.
+__device__ __forceinline__ void scan_256(const uint32_t *in, uint32_t *out, uint32_t *warp_sums) {
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t v = 0, incl = 0;
+  if (threadIdx.x < SORT_RADIX) {
+    v = in[threadIdx.x];
+    incl = v;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const uint32_t u = __shfl_up_sync(0xffffffffu, incl, off);
+      if (lane >= (unsigned)off)
+        incl += u;
+    }
+    if (lane == 31)
+      warp_sums[warp] = incl;
+  }
+  __syncthreads();
+  if (threadIdx.x < SORT_RADIX) {
+    uint32_t before = 0;
+    for (unsigned k = 0; k < warp; k++)
+      before += warp_sums[k];
+    out[threadIdx.x] = before + incl - v;
+  }
+  __syncthreads();
+}
+
+// Scatter one tile: `count` items at seg + base of a segment whose digit totals
+// are seg_totals[0..255]; tile_counts[d * count_stride] is this tile's exclusive
+// prefix over the segment's earlier tiles for digit d.  Ranks among equal digits: STABLE (every pass after the
+// first, which LSD order requires) ranks warp by warp, 32 consecutive items
+// per round with __match_any_sync; the first pass may take any order and
+// ranks with shared atomics.  The tile is then reordered in shared memory so
+// that each digit's run is written to global memory with consecutive
+// addresses.
+template <bool STABLE>
+__device__ __forceinline__ void sort_scatter_tile(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
+                                                  uint32_t *__restrict__ keys_out, uint32_t *__restrict__ vals_out, size_t seg, unsigned base,
+                                                  unsigned count, unsigned shift, const uint32_t *__restrict__ tile_counts, size_t count_stride,
+                                                  const uint32_t *__restrict__ seg_totals) {
+  __shared__ uint32_t s_key[SORT_TILE];
+  __shared__ uint32_t s_val[SORT_TILE];
+  __shared__ uint32_t whist[STABLE ? SORT_WARPS : 1][SORT_RADIX];
+  __shared__ uint32_t tile_cnt[SORT_RADIX], tile_off[SORT_RADIX], glob[SORT_RADIX], digit_base[SORT_RADIX], warp_sums[SORT_WARPS];
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned sub = warp * (32 * SORT_ITEMS); // this warp's items: base + sub + r*32 + lane
+  if (STABLE) {
+    for (unsigned d = lane; d < SORT_RADIX; d += 32)
+      whist[warp][d] = 0;
+  } else {
+    for (unsigned d = threadIdx.x; d < SORT_RADIX; d += blockDim.x)
+      tile_cnt[d] = 0;
+  }
+  __syncthreads();
+  uint32_t key[SORT_ITEMS], val[SORT_ITEMS], rank[SORT_ITEMS];
+  const unsigned lt_mask = (1u << lane) - 1;
+#pragma unroll
+  for (unsigned r = 0; r < SORT_ITEMS; r++) {
+    const unsigned i = sub + r * 32 + lane;
+    const bool valid = i < count;
+    key[r] = valid ? keys_in[seg + base + i] : 0;
+    val[r] = valid ? vals_in[seg + base + i] : 0;
+    const unsigned d = valid ? sort_digit(key[r], shift) : SORT_RADIX;
+    if (STABLE) {
+      const unsigned peers = __match_any_sync(0xffffffffu, d);
+      const uint32_t before = valid ? whist[warp][d] : 0;
+      __syncwarp();
+      if (valid && lane == (unsigned)(__ffs(peers) - 1))
+        whist[warp][d] = before + __popc(peers);
+      __syncwarp();
+      rank[r] = before + __popc(peers & lt_mask);
+    } else {
+      rank[r] = valid ? atomicAdd(&tile_cnt[d], 1u) : 0;
+    }
+  }
+  __syncthreads();
+  if (STABLE) {
+    // per digit: exclusive prefix over warps (warp order = item order)
+    for (unsigned d = threadIdx.x; d < SORT_RADIX; d += blockDim.x) {
+      uint32_t run = 0;
+#pragma unroll
+      for (unsigned k = 0; k < SORT_WARPS; k++) {
+        const uint32_t t = whist[k][d];
+        whist[k][d] = run;
+        run += t;
+      }
+      tile_cnt[d] = run;
+    }
+    __syncthreads();
+  }
+  scan_256(tile_cnt, tile_off, warp_sums);
+  for (unsigned d = threadIdx.x; d < SORT_RADIX; d += blockDim.x)
+    glob[d] = seg_totals[d];
+  __syncthreads();
+  scan_256(glob, digit_base, warp_sums); // digit bases of this segment
+  for (unsigned d = threadIdx.x; d < SORT_RADIX; d += blockDim.x)
+    glob[d] = digit_base[d] + tile_counts[d * count_stride];
+#pragma unroll
+  for (unsigned r = 0; r < SORT_ITEMS; r++) {
+    const unsigned i = sub + r * 32 + lane;
+    if (i < count) {
+      const unsigned d = sort_digit(key[r], shift);
+      const unsigned pos = tile_off[d] + (STABLE ? whist[warp][d] : 0) + rank[r];
+      s_key[pos] = key[r];
+      s_val[pos] = val[r];
+    }
+  }
+  __syncthreads();
+#pragma unroll 4
+  for (unsigned j = 0; j < SORT_ITEMS; j++) {
+    const unsigned pos = j * SORT_THREADS + threadIdx.x;
+    if (pos < count) {
+      const uint32_t k = s_key[pos];
+      const unsigned d = sort_digit(k, shift);
+      const size_t out = seg + glob[d] + (pos - tile_off[d]);
+      keys_out[out] = k;
+      vals_out[out] = s_val[pos];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// accumulation helpers
+// ---------------------------------------------------------------------------
+// 16-byte asynchronous global -> shared copies (L2 only: bases are not reused
+// by the same SM), one commit group per base point.
+__device__ __forceinline__ void cp_async_16(void *smem, const void *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int PENDING> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(PENDING) : "memory"); }
+
+
+#ifndef ACC_MIN_BLOCKS
+#define ACC_MIN_BLOCKS 4 // resident accumulation blocks per SM (caps registers at 128)
+#endif
+
+// Bucket accumulation over a list of segments of sorted (key, value) entries.
+// The nonzero entries of all segments form one virtual list of M entries,
+// split into equal contiguous ranges, one per thread (total_threads).  Each
+// thread walks its range, gathers the signed affine base of every entry
+// (double-buffered through shared memory by cp.async), starts a new XYZZ
+// accumulator when the bucket changes and otherwise does one mixed addition.
+// A bucket that starts inside the range is written directly (and flagged); a
+// bucket continued from the previous range leaves a "head" partial sum for
+// merge_heads_kernel.  SEG describes the segments (all methods device-side):
+//   count()          segments
+//   prefix(s)        nonzero entries before segment s (s <= count())
+//   first(s), end(s) physical index of the first nonzero entry / one past the last
+//   empty(s)         no nonzero entry
+//   bucket(s, key)   global bucket slot of a key of segment s
+//   base(s, val)     affine base of a value of segment s (sign bit ignored)
+template <class SEG>
+__device__ __forceinline__ void accumulate_ranges(const SEG &seg, const uint32_t *__restrict__ keys, const uint32_t *__restrict__ vals,
+                                                  unsigned total_threads, xyzz *__restrict__ buckets, uint8_t *__restrict__ flags,
+                                                  uint32_t *__restrict__ head_bucket, xyzz *__restrict__ head_point,
+                                                  uint4 (*s_base)[4][ACC_THREADS]) {
+  const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= total_threads)
+    return;
+  // Only the first min(total, total_threads) ranges are used, so every active
+  // range holds at least one entry and the heads of one bucket stay
+  // contiguous (an empty range between them would let two merge threads
+  // update the same bucket).
+  const unsigned segments = seg.count();
+  const unsigned long long total = seg.prefix(segments);
+  const unsigned long long active = total < total_threads ? total : total_threads;
+  head_bucket[t] = INVALID_BUCKET;
+  if (t >= active)
+    return;
+  const unsigned long long beg = total * t / active;
+  const unsigned long long end = total * (t + 1) / active;
+  unsigned w = 0;
+  while (w + 1 < segments && seg.prefix(w + 1) <= beg)
+    w++;
+  // cursor: physical index, its segment, and the end of that segment
+  size_t idx = seg.first(w) + (size_t)(beg - seg.prefix(w));
+  unsigned cw = w;
+  size_t seg_end = seg.end(w);
+  auto advance = [&]() {
+    idx++;
+    if (idx == seg_end) {
+      unsigned s = cw + 1;
+      while (s < segments && seg.empty(s))
+        s++;
+      cw = s;
+      if (s < segments) {
+        seg_end = seg.end(s);
+        idx = seg.first(s);
+      }
+    }
+  };
+
+  auto issue = [&](unsigned slot, unsigned s, uint32_t val) {
+    const uint4 *src = reinterpret_cast<const uint4 *>(seg.base(s, val));
+#pragma unroll
+    for (int c = 0; c < 4; c++)
+      cp_async_16(&s_base[slot][c][threadIdx.x], src + c);
+    cp_async_commit();
+  };
+  // A base's y is never 0 (BN254 G1 has odd order, so no point has y = 0):
+  // its negation is 2p - y.
+  auto fetch = [&](unsigned slot, uint32_t val) {
+    affine p;
+    uint32_t *w32 = reinterpret_cast<uint32_t *>(&p);
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      const uint4 v = s_base[slot][c][threadIdx.x];
+      w32[4 * c + 0] = v.x;
+      w32[4 * c + 1] = v.y;
+      w32[4 * c + 2] = v.z;
+      w32[4 * c + 3] = v.w;
+    }
+    const fe ny = fq::neg_nonzero(p.y);
+    const bool negative = val >> 31;
+#pragma unroll
+    for (int i = 0; i < 8; i++)
+      p.y.l[i] = negative ? ny.l[i] : p.y.l[i];
+    return p;
+  };
+
+  // entry 0 of the range
+  uint32_t key = keys[idx];
+  uint32_t val = vals[idx];
+  issue(0, cw, val);
+  // does this range start in the middle of a bucket?
+  const bool continued = idx > seg.first(w) && keys[idx - 1] == key;
+  unsigned bucket = seg.bucket(w, key);
+  const unsigned long long count = end - beg;
+  // entry 1 is fetched before entry 0 is consumed
+  uint32_t nkey = 0, nval = 0;
+  unsigned nw = 0;
+  if (count > 1) {
+    advance();
+    nkey = keys[idx];
+    nval = vals[idx];
+    nw = cw;
+    issue(1, nw, nval);
+    cp_async_wait<1>();
+  } else {
+    cp_async_wait<0>();
+  }
+  xyzz acc = curve::from_affine(fetch(0, val));
+  bool acc_inf = false; // a partial sum can cancel to infinity (p + (-p))
+  bool first = true;
+  for (unsigned long long k = 1; k < count; k++) {
+    key = nkey;
+    val = nval;
+    const unsigned kw = nw;
+    const unsigned slot = (unsigned)(k & 1);
+    if (k + 1 < count) {
+      advance();
+      nkey = keys[idx];
+      nval = vals[idx];
+      nw = cw;
+      issue(slot ^ 1, nw, nval);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    const affine p = fetch(slot, val);
+    const unsigned b = seg.bucket(kw, key);
+    if (b != bucket) {
+      if (acc_inf)
+        acc = curve::infinity();
+      if (first && continued) {
+        head_bucket[t] = bucket;
+        store_xyzz(head_point + t, acc);
+      } else {
+        store_xyzz(buckets + bucket, acc);
+        flags[bucket] = 1;
+      }
+      first = false;
+      bucket = b;
+      acc = curve::from_affine(p);
+      acc_inf = false;
+    } else if (acc_inf) {
+      acc = curve::from_affine(p);
+      acc_inf = false;
+    } else {
+      acc = curve::add_affine_finite(acc, p, acc_inf);
+    }
+  }
+  if (acc_inf)
+    acc = curve::infinity();
+  if (first && continued) {
+    head_bucket[t] = bucket;
+    store_xyzz(head_point + t, acc);
+  } else {
+    store_xyzz(buckets + bucket, acc);
+    flags[bucket] = 1;
+  }
+}
+
+} // namespace msm_b200

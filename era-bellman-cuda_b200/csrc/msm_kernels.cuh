@@ -127,4 +127,13 @@ __global__ void gather_results_kernel(const xyzz *__restrict__ streams, const xy
 // stride of the per-window plain-sum streams (stream 0: G entries, stream s: G >> s)
 __host__ __device__ __forceinline__ size_t stream_stride(unsigned log_g) { return (size_t)2 << log_g; }
 
+// Stream layout per window (stride 2G): stream 0 = the G group sums "acc",
+// stream s >= 1 = the G >> s odd entries of tree level s - 1.
+__host__ __device__ __forceinline__ unsigned stream_offset(unsigned log_g, unsigned s) {
+  const unsigned g = 1u << log_g;
+  return s == 0 ? 0 : g + (g - (g >> (s - 1)));
+}
+
+__host__ __device__ __forceinline__ unsigned stream_length(unsigned log_g, unsigned s) { return s == 0 ? (1u << log_g) : (1u << log_g) >> s; }
+
 } // namespace msm_b200

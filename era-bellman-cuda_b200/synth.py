@@ -108,3 +108,22 @@ def workload(name: str, n: int, seed: int):
     else:
         raise ValueError(name)
     return s, base_multipliers(seed, n)
+
+
+def batch_lengths(seed: int, instances: int, lo_log: int = 10, hi_log: int = 22) -> np.ndarray:
+    """Instance lengths log-uniform in [2^lo_log, 2^hi_log], rounded to integers
+    (config 3: 64 instances in [2^10, 2^22], seed 3).  Stream 4."""
+    u = (_bitgen(seed, 4).random_raw(instances).astype(np.uint64) >> np.uint64(11)).astype(np.float64) / float(1 << 53)
+    return np.rint(np.exp2(lo_log + (hi_log - lo_log) * u)).astype(np.int64)
+
+
+def batch_workload(seed: int, lengths) -> list:
+    """Per instance k: (distribution, Montgomery scalars); even k uniform, odd k
+    skewed (the config-2 mix), instance k drawn from seed * 1000 + k.  All
+    instances use prefixes of one base table (base_multipliers of the table)."""
+    out = []
+    for k, n in enumerate(lengths):
+        dist = "uniform" if k % 2 == 0 else "skewed"
+        sub = seed * 1000 + k
+        out.append((dist, uniform_scalars(sub, int(n)) if dist == "uniform" else skewed_scalars(sub, int(n))))
+    return out

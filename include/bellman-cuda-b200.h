@@ -72,6 +72,50 @@ bc_error msm_b200_default_window_bits(unsigned count, unsigned *window_bits);
  * memory.  Used to build synthetic base tables on the device. */
 bc_error msm_b200_generator_multiples_async(const void *k, void *bases, unsigned count, bc_stream stream);
 
+/* ---- Batched MSMs over one resident base table (no counterpart in the
+ * reference).
+ *
+ * A base table keeps `count` affine points (Montgomery form, 64 B each) on the
+ * device together with their precomputed window multiples 2^(c j) P_i for one
+ * or more window widths c, so that an MSM over a prefix of the table needs a
+ * single set of 2^(c-1) buckets.  A batch is a fixed list of instance lengths
+ * (each a prefix of the table); all its instances run as one kernel chain over
+ * a shared work list, captured once in a CUDA graph and replayed by every
+ * execution.  Results follow the msm_execute_async convention (254 Jacobian
+ * points per instance, MSM = sum_i 2^i R_i; here R_i = 0 for i >= c). */
+#define MSM_B200_MAX_BATCH 256u
+typedef struct msm_b200_base_table_t *msm_b200_base_table;
+typedef struct msm_b200_batch_t *msm_b200_batch;
+
+/* Builds a table from `bases` (device or host memory; copied).  window_bits:
+ * the widths to precompute (widths entries, 2..24); with widths = 0 the widths
+ * msm_b200_batch_window_bits picks for every length up to `count`, each only
+ * for the prefix that lengths of that width can reach.  Synchronous on
+ * `stream`; the table owns its device memory until destroyed. */
+bc_error msm_b200_base_table_create(msm_b200_base_table *table, const void *bases, unsigned count, const unsigned *window_bits, unsigned widths,
+                                    bc_stream stream);
+/* Device bytes the table holds. */
+bc_error msm_b200_base_table_bytes(msm_b200_base_table table, size_t *bytes);
+bc_error msm_b200_base_table_destroy(msm_b200_base_table table);
+
+/* The window width the batched path uses for an instance of `count` points:
+ * the checked-in table written by the autotuner (era-bellman-cuda_b200/autotune.py). */
+bc_error msm_b200_batch_window_bits(unsigned count, unsigned *window_bits);
+
+/* Plans a batch of `instances` (1..MSM_B200_MAX_BATCH) MSMs of counts[k]
+ * points over the first counts[k] points of `table`; window_bits (optional, 0
+ * entries = tuned) forces per-instance widths, which the table must hold.
+ * Allocates the batch's scratch (cudaMalloc) and captures its CUDA graph. */
+bc_error msm_b200_batch_create(msm_b200_batch *batch, msm_b200_base_table table, const unsigned *counts, unsigned instances,
+                               const unsigned *window_bits);
+/* Runs the batch: scalars[k] (counts[k] Montgomery-form scalars) and
+ * results[k] (254 Jacobian points) are device pointers.  Executions of one
+ * batch share its scratch: serialise them (one stream). */
+bc_error msm_b200_batch_execute_async(msm_b200_batch batch, const void *const *scalars, void *const *results, bc_stream stream);
+/* Scratch bytes, kernels in the graph, and (window, point) entries of a batch. */
+bc_error msm_b200_batch_info(msm_b200_batch batch, size_t *scratch_bytes, unsigned *kernels, unsigned long long *entries);
+bc_error msm_b200_batch_destroy(msm_b200_batch batch);
+
 /* An MSM that allocates no memory (no counterpart in the reference).
  *
  * For callers that cannot allocate device memory at call time: code running
