@@ -23,9 +23,11 @@
 #include "batch_tuning.h"
 #include "bellman-cuda-b200.h"
 #include "msm_device.cuh"
+#include "msm_batch.cuh"
 #include "msm_host.cuh"
 
 #include <algorithm>
+#include <cstring>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -41,8 +43,6 @@ namespace msm_b200 {
       return check_result_;                                                                                                                    \
   } while (0)
 
-constexpr unsigned MAX_BATCH = MSM_B200_MAX_BATCH;
-constexpr unsigned MAX_TABLE_BITS = 24;
 constexpr unsigned IO_CHUNK = 64; // instances per descriptor-update launch
 
 static unsigned ceil_log2_u(unsigned long long v) {
@@ -53,6 +53,8 @@ static unsigned ceil_log2_u(unsigned long long v) {
 }
 
 static unsigned windows_for(unsigned c) { return (RESULT_BITS + c - 1) / c; }
+
+static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
 
 unsigned batch_window_bits(unsigned n) {
   const unsigned lg = ceil_log2_u(n);
@@ -65,20 +67,7 @@ unsigned batch_window_bits(unsigned n) {
 // ---------------------------------------------------------------------------
 // device descriptors
 // ---------------------------------------------------------------------------
-struct batch_instance {
-  unsigned long long entry_offset; // first entry of the instance's segment
-  const affine *table;             // M_c: table[j * stride + i] = 2^(c j) P_i
-  unsigned n, c, windows, stride;
-  unsigned entries;     // windows * n
-  unsigned tiles;       // sort tiles of the segment
-  unsigned tile_base;   // first global sort tile of the segment
-  unsigned bucket_base; // first bucket slot (slot 0 holds |d| = 2^(c-1))
-};
 
-struct batch_io {
-  const fe *scalars; // n Montgomery-form scalars (device)
-  jacobian *results; // 254 Jacobian points (device)
-};
 
 struct batch_io_update {
   batch_io io[IO_CHUNK];
@@ -260,18 +249,6 @@ __global__ void batch_gather_kernel(const xyzz *__restrict__ streams, const xyzz
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
-struct base_table_impl {
-  int device = 0;
-  unsigned count = 0;
-  affine *mult[MAX_TABLE_BITS + 1] = {}; // mult[c]: windows_for(c) * prefix[c] points, or null
-  unsigned prefix[MAX_TABLE_BITS + 1] = {};
-  size_t bytes = 0;
-  ~base_table_impl() {
-    for (affine *m : mult)
-      if (m)
-        cudaFree(m);
-  }
-};
 
 // Builds M_c for the first `prefix` points of `bases` (device memory).
 static cudaError_t build_multiples(base_table_impl &t, unsigned c, unsigned prefix, const affine *bases, cudaStream_t stream) {
@@ -340,68 +317,137 @@ cudaError_t base_table_create(base_table_impl **out, const void *bases, unsigned
   return cudaSuccess;
 }
 
-struct batch_group {
-  unsigned c;
-  std::vector<unsigned> members; // instances, in bucket order
-  plan p;                        // reduction geometry (windows = members)
-  unsigned bucket_base;
-  size_t tree[2], streams[2], members_dev;
-};
 
-struct batch_impl {
-  int device = 0;
-  const base_table_impl *table = nullptr;
-  unsigned instances = 0;
-  unsigned long long total_entries = 0;
-  unsigned total_points = 0, total_tiles = 0, slots = 0, sort_passes = 0, acc_threads = 0;
-  std::vector<batch_instance> inst;
-  std::vector<batch_group> groups;
-  uint8_t *scratch = nullptr;
-  size_t scratch_bytes = 0;
-  size_t keys[2], vals[2], counts, totals, zeros, buckets, flags, hb[2], hp[2], inst_dev, point_offset, tile_seg, io;
-  cudaStream_t capture = nullptr;
-  std::vector<cudaStream_t> forks;
-  std::vector<cudaEvent_t> fork_events;
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
-  unsigned launches = 0;
-  ~batch_impl() {
-    if (exec)
-      cudaGraphExecDestroy(exec);
-    if (graph)
-      cudaGraphDestroy(graph);
-    for (cudaEvent_t e : fork_events)
-      cudaEventDestroy(e);
-    for (cudaStream_t s : forks)
-      cudaStreamDestroy(s);
-    if (capture)
-      cudaStreamDestroy(capture);
-    if (scratch)
-      cudaFree(scratch);
+
+cudaError_t make_batch_plan(batch_plan &b, const base_table_impl *table, const unsigned *counts, unsigned instances, const unsigned *window_bits,
+                            int sms) {
+  if (!table || !counts || instances == 0 || instances > MAX_BATCH)
+    return cudaErrorInvalidValue;
+  b = batch_plan{};
+  b.instances = instances;
+  b.inst.resize(instances);
+  b.point_offset.assign(instances + 1, 0);
+  // instance geometry; reduction groups by window width (buckets of a group contiguous)
+  std::map<unsigned, std::vector<unsigned>> by_c;
+  unsigned max_c = 0;
+  unsigned long long points = 0;
+  for (unsigned k = 0; k < instances; k++) {
+    const unsigned n = counts[k];
+    const unsigned c = window_bits && window_bits[k] ? window_bits[k] : batch_window_bits(n);
+    if (n == 0 || c < 2 || c > MAX_TABLE_BITS || !table->mult[c] || n > table->prefix[c])
+      return cudaErrorInvalidValue;
+    batch_instance &d = b.inst[k];
+    d.n = n;
+    d.c = c;
+    d.windows = windows_for(c);
+    d.stride = table->prefix[c];
+    d.table = table->mult[c];
+    if ((unsigned long long)d.windows * n >= (1ull << 31) || d.windows * (unsigned long long)d.stride >= (1ull << 31))
+      return cudaErrorInvalidValue;
+    d.entries = d.windows * n;
+    d.entry_offset = b.total_entries;
+    d.tiles = (d.entries + SORT_TILE - 1) / SORT_TILE;
+    d.tile_base = b.total_tiles;
+    b.total_entries += d.entries;
+    b.total_tiles += d.tiles;
+    b.point_offset[k] = (unsigned)points;
+    points += n;
+    max_c = std::max(max_c, c);
+    by_c[c].push_back(k);
   }
-  template <class T> T *at(size_t off) const { return reinterpret_cast<T *>(scratch + off); }
-};
+  if (points >= (1ull << 32) || b.total_tiles >= (1u << 31))
+    return cudaErrorInvalidValue;
+  b.point_offset[instances] = (unsigned)points;
+  b.total_points = (unsigned)points;
+  b.sort_passes = (max_c + SORT_RADIX_BITS - 1) / SORT_RADIX_BITS;
+  for (auto &kv : by_c) {
+    batch_group g;
+    g.c = kv.first;
+    g.members = kv.second;
+    g.bucket_base = b.slots;
+    g.p = make_plan(1, g.c, sms);
+    g.p.windows = (unsigned)g.members.size();
+    for (unsigned w = 0; w < g.members.size(); w++)
+      b.inst[g.members[w]].bucket_base = b.slots + (w << (g.c - 1));
+    b.slots += (unsigned)g.members.size() << (g.c - 1);
+    b.groups.push_back(g);
+  }
+  b.tile_seg.resize(b.total_tiles);
+  for (unsigned k = 0; k < instances; k++)
+    std::fill(b.tile_seg.begin() + b.inst[k].tile_base, b.tile_seg.begin() + b.inst[k].tile_base + b.inst[k].tiles, k);
+  const unsigned long long full = (unsigned long long)sms * ACC_MIN_BLOCKS * ACC_THREADS;
+  b.acc_threads = (unsigned)std::max(1ull, std::min(full, (b.total_entries + 7) / 8));
+  // scratch layout
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    const size_t at = off;
+    off += align256(bytes);
+    return at;
+  };
+  for (int i = 0; i < 2; i++) {
+    b.keys[i] = take(b.total_entries * 4);
+    b.vals[i] = take(b.total_entries * 4);
+  }
+  b.counts = take((size_t)b.total_tiles * SORT_RADIX * 4);
+  b.totals = take((size_t)instances * SORT_RADIX * 4);
+  b.zeros = take((size_t)instances * 4);
+  b.buckets = take((size_t)b.slots * sizeof(xyzz));
+  b.flags = take(b.slots);
+  for (int i = 0; i < 2; i++) {
+    b.hb[i] = take((size_t)b.acc_threads * 4);
+    b.hp[i] = take((size_t)b.acc_threads * sizeof(xyzz));
+  }
+  for (batch_group &g : b.groups)
+    for (int i = 0; i < 2; i++) {
+      g.tree[i] = take(((size_t)g.p.windows << g.p.log_g) * sizeof(xyzz));
+      g.streams[i] = take((size_t)g.p.windows * stream_stride(g.p.log_g) * sizeof(xyzz));
+    }
+  b.io = take(instances * sizeof(batch_io));
+  // constant descriptors last, in one contiguous range (one upload)
+  b.descriptors = off;
+  b.inst_dev = take(instances * sizeof(batch_instance));
+  b.point_offset_dev = take((instances + 1) * 4);
+  b.tile_seg_dev = take((size_t)b.total_tiles * 4);
+  for (batch_group &g : b.groups)
+    g.members_dev = take(g.members.size() * 4);
+  b.bytes = off;
+  return cudaSuccess;
+}
 
-static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
+// The constant descriptors as they lie in scratch from b.descriptors on.
+std::vector<uint8_t> descriptor_image(const batch_plan &b) {
+  std::vector<uint8_t> img(b.bytes - b.descriptors, 0);
+  auto put = [&](size_t off, const void *src, size_t bytes) { std::memcpy(img.data() + (off - b.descriptors), src, bytes); };
+  put(b.inst_dev, b.inst.data(), b.instances * sizeof(batch_instance));
+  put(b.point_offset_dev, b.point_offset.data(), (b.instances + 1) * 4);
+  put(b.tile_seg_dev, b.tile_seg.data(), b.tile_seg.size() * 4);
+  for (const batch_group &g : b.groups)
+    put(g.members_dev, g.members.data(), g.members.size() * 4);
+  return img;
+}
 
-// Enqueues the whole chain on b.capture (and its forks for the reductions).
-static cudaError_t enqueue_batch(batch_impl &b) {
-  cudaStream_t s = b.capture;
+// Enqueues the chain of plan b over `scratch` on stream s.  With forks (one
+// stream and one event per reduction group, plus one event), the per-width
+// reductions run concurrently; otherwise one after another on s.
+cudaError_t enqueue_batch(const batch_plan &b, uint8_t *scratch, cudaStream_t s, const cudaStream_t *forks, const cudaEvent_t *fork_events,
+                                 unsigned *launches) {
+  auto at = [&](size_t off) { return scratch + off; };
   unsigned launched = 0;
-  uint32_t *keys[2] = {b.at<uint32_t>(b.keys[0]), b.at<uint32_t>(b.keys[1])};
-  uint32_t *vals[2] = {b.at<uint32_t>(b.vals[0]), b.at<uint32_t>(b.vals[1])};
-  const batch_instance *inst = b.at<batch_instance>(b.inst_dev);
-  const batch_io *io = b.at<batch_io>(b.io);
-  uint32_t *counts = b.at<uint32_t>(b.counts), *totals = b.at<uint32_t>(b.totals), *zeros = b.at<uint32_t>(b.zeros);
-  const unsigned *tile_seg = b.at<unsigned>(b.tile_seg);
-  xyzz *buckets = b.at<xyzz>(b.buckets);
-  uint8_t *flags = b.at<uint8_t>(b.flags);
-  uint32_t *hb[2] = {b.at<uint32_t>(b.hb[0]), b.at<uint32_t>(b.hb[1])};
-  xyzz *hp[2] = {b.at<xyzz>(b.hp[0]), b.at<xyzz>(b.hp[1])};
+  uint32_t *keys[2] = {reinterpret_cast<uint32_t *>(at(b.keys[0])), reinterpret_cast<uint32_t *>(at(b.keys[1]))};
+  uint32_t *vals[2] = {reinterpret_cast<uint32_t *>(at(b.vals[0])), reinterpret_cast<uint32_t *>(at(b.vals[1]))};
+  const batch_instance *inst = reinterpret_cast<const batch_instance *>(at(b.inst_dev));
+  const batch_io *io = reinterpret_cast<const batch_io *>(at(b.io));
+  uint32_t *counts = reinterpret_cast<uint32_t *>(at(b.counts)), *totals = reinterpret_cast<uint32_t *>(at(b.totals)),
+           *zeros = reinterpret_cast<uint32_t *>(at(b.zeros));
+  const unsigned *tile_seg = reinterpret_cast<const unsigned *>(at(b.tile_seg_dev));
+  xyzz *buckets = reinterpret_cast<xyzz *>(at(b.buckets));
+  uint8_t *flags = at(b.flags);
+  uint32_t *hb[2] = {reinterpret_cast<uint32_t *>(at(b.hb[0])), reinterpret_cast<uint32_t *>(at(b.hb[1]))};
+  xyzz *hp[2] = {reinterpret_cast<xyzz *>(at(b.hp[0])), reinterpret_cast<xyzz *>(at(b.hp[1]))};
 
   CHECK(cudaMemsetAsync(flags, 0, b.slots, s));
-  batch_digits_kernel<<<(b.total_points + 255) / 256, 256, 0, s>>>(inst, b.at<unsigned>(b.point_offset), b.instances, b.total_points, io, keys[0],
-                                                                   vals[0]);
+  batch_digits_kernel<<<(b.total_points + 255) / 256, 256, 0, s>>>(inst, reinterpret_cast<const unsigned *>(at(b.point_offset_dev)), b.instances,
+                                                                   b.total_points, io, keys[0], vals[0]);
   CHECK(cudaGetLastError());
   launched++;
   int cur = 0;
@@ -438,17 +484,18 @@ static cudaError_t enqueue_batch(batch_impl &b) {
     heads = out;
     h ^= 1;
   }
-  // reductions: one chain per window width, each on its own forked stream
-  CHECK(cudaEventRecord(b.fork_events[0], s));
+  if (forks)
+    CHECK(cudaEventRecord(fork_events[0], s));
   for (size_t g = 0; g < b.groups.size(); g++) {
     const batch_group &grp = b.groups[g];
     const plan &p = grp.p;
-    cudaStream_t fs = b.forks[g];
-    CHECK(cudaStreamWaitEvent(fs, b.fork_events[0], 0));
+    cudaStream_t fs = forks ? forks[g] : s;
+    if (forks)
+      CHECK(cudaStreamWaitEvent(fs, fork_events[0], 0));
     xyzz *gb = buckets + grp.bucket_base;
     const uint8_t *gf = flags + grp.bucket_base;
-    xyzz *tree[2] = {b.at<xyzz>(grp.tree[0]), b.at<xyzz>(grp.tree[1])};
-    xyzz *streams[2] = {b.at<xyzz>(grp.streams[0]), b.at<xyzz>(grp.streams[1])};
+    xyzz *tree[2] = {reinterpret_cast<xyzz *>(at(grp.tree[0])), reinterpret_cast<xyzz *>(at(grp.tree[1]))};
+    xyzz *streams[2] = {reinterpret_cast<xyzz *>(at(grp.streams[0])), reinterpret_cast<xyzz *>(at(grp.streams[1]))};
     const unsigned group_threads = p.windows << p.log_g;
     reduce_groups_kernel<<<(group_threads + ACC_THREADS - 1) / ACC_THREADS, ACC_THREADS, 0, fs>>>(gb, gf, p.windows, p.log_b, p.log_m, tree[0],
                                                                                                    streams[0]);
@@ -475,161 +522,26 @@ static cudaError_t enqueue_batch(batch_impl &b) {
       si ^= 1;
     }
     const unsigned gather_threads = p.windows * RESULT_BITS;
-    batch_gather_kernel<<<(gather_threads + 127) / 128, 128, 0, fs>>>(streams[si], gb, gf, b.at<unsigned>(grp.members_dev), p.windows, p.c,
-                                                                      p.log_m, p.log_g, io);
+    batch_gather_kernel<<<(gather_threads + 127) / 128, 128, 0, fs>>>(streams[si], gb, gf, reinterpret_cast<const unsigned *>(at(grp.members_dev)),
+                                                                      p.windows, p.c, p.log_m, p.log_g, io);
     CHECK(cudaGetLastError());
     launched++;
-    CHECK(cudaEventRecord(b.fork_events[g + 1], fs));
-    CHECK(cudaStreamWaitEvent(s, b.fork_events[g + 1], 0));
-  }
-  b.launches = launched;
-  return cudaSuccess;
-}
-
-cudaError_t batch_create(batch_impl **out, const base_table_impl *table, const unsigned *counts, unsigned instances, const unsigned *window_bits) {
-  if (!out || !table || !counts || instances == 0 || instances > MAX_BATCH)
-    return cudaErrorInvalidValue;
-  int device = 0;
-  CHECK(cudaGetDevice(&device));
-  if (device != table->device)
-    return cudaErrorInvalidDevice;
-  int sms = 0;
-  CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-  batch_impl *bp = new (std::nothrow) batch_impl;
-  if (!bp)
-    return cudaErrorMemoryAllocation;
-  std::unique_ptr<batch_impl> owner(bp);
-  batch_impl &b = *bp;
-  b.device = device;
-  b.table = table;
-  b.instances = instances;
-  b.inst.resize(instances);
-  // instance geometry; reduction groups by window width (buckets of a group contiguous)
-  std::map<unsigned, std::vector<unsigned>> by_c;
-  unsigned max_c = 0;
-  std::vector<unsigned> point_offset(instances + 1, 0);
-  unsigned long long points = 0;
-  for (unsigned k = 0; k < instances; k++) {
-    const unsigned n = counts[k];
-    const unsigned c = window_bits && window_bits[k] ? window_bits[k] : batch_window_bits(n);
-    if (n == 0 || c < 2 || c > MAX_TABLE_BITS || !table->mult[c] || n > table->prefix[c])
-      return cudaErrorInvalidValue;
-    batch_instance &d = b.inst[k];
-    d.n = n;
-    d.c = c;
-    d.windows = windows_for(c);
-    d.stride = table->prefix[c];
-    d.table = table->mult[c];
-    d.entries = d.windows * n;
-    d.entry_offset = b.total_entries;
-    d.tiles = (d.entries + SORT_TILE - 1) / SORT_TILE;
-    d.tile_base = b.total_tiles;
-    if ((unsigned long long)d.windows * n >= (1ull << 31) || d.windows * (unsigned long long)d.stride >= (1ull << 31))
-      return cudaErrorInvalidValue;
-    b.total_entries += d.entries;
-    b.total_tiles += d.tiles;
-    point_offset[k] = (unsigned)points;
-    points += n;
-    max_c = std::max(max_c, c);
-    by_c[c].push_back(k);
-  }
-  if (points >= (1ull << 32) || b.total_tiles >= (1u << 31))
-    return cudaErrorInvalidValue;
-  point_offset[instances] = (unsigned)points;
-  b.total_points = (unsigned)points;
-  b.sort_passes = (max_c + SORT_RADIX_BITS - 1) / SORT_RADIX_BITS;
-  for (auto &kv : by_c) {
-    batch_group g;
-    g.c = kv.first;
-    g.members = kv.second;
-    g.bucket_base = b.slots;
-    g.p = make_plan(1, g.c, sms);
-    g.p.windows = (unsigned)g.members.size();
-    for (unsigned w = 0; w < g.members.size(); w++)
-      b.inst[g.members[w]].bucket_base = b.slots + (w << (g.c - 1));
-    b.slots += (unsigned)g.members.size() << (g.c - 1);
-    b.groups.push_back(g);
-  }
-  const unsigned long long full = (unsigned long long)sms * ACC_MIN_BLOCKS * ACC_THREADS;
-  b.acc_threads = (unsigned)std::max(1ull, std::min(full, (b.total_entries + 7) / 8));
-  // scratch layout
-  size_t off = 0;
-  auto take = [&](size_t bytes) {
-    const size_t at = off;
-    off += align256(bytes);
-    return at;
-  };
-  for (int i = 0; i < 2; i++) {
-    b.keys[i] = take(b.total_entries * 4);
-    b.vals[i] = take(b.total_entries * 4);
-  }
-  b.counts = take((size_t)b.total_tiles * SORT_RADIX * 4);
-  b.totals = take((size_t)instances * SORT_RADIX * 4);
-  b.zeros = take((size_t)instances * 4);
-  b.buckets = take((size_t)b.slots * sizeof(xyzz));
-  b.flags = take(b.slots);
-  for (int i = 0; i < 2; i++) {
-    b.hb[i] = take((size_t)b.acc_threads * 4);
-    b.hp[i] = take((size_t)b.acc_threads * sizeof(xyzz));
-  }
-  for (batch_group &g : b.groups) {
-    for (int i = 0; i < 2; i++) {
-      g.tree[i] = take(((size_t)g.p.windows << g.p.log_g) * sizeof(xyzz));
-      g.streams[i] = take((size_t)g.p.windows * stream_stride(g.p.log_g) * sizeof(xyzz));
+    if (forks) {
+      CHECK(cudaEventRecord(fork_events[g + 1], fs));
+      CHECK(cudaStreamWaitEvent(s, fork_events[g + 1], 0));
     }
-    g.members_dev = take(g.members.size() * 4);
   }
-  b.inst_dev = take(instances * sizeof(batch_instance));
-  b.point_offset = take((instances + 1) * 4);
-  b.tile_seg = take((size_t)b.total_tiles * 4);
-  b.io = take(instances * sizeof(batch_io));
-  b.scratch_bytes = off;
-  CHECK(cudaMalloc(&b.scratch, b.scratch_bytes));
-  // constant descriptors
-  std::vector<unsigned> tile_seg(b.total_tiles);
-  for (unsigned k = 0; k < instances; k++)
-    std::fill(tile_seg.begin() + b.inst[k].tile_base, tile_seg.begin() + b.inst[k].tile_base + b.inst[k].tiles, k);
-  CHECK(cudaMemcpy(b.scratch + b.inst_dev, b.inst.data(), instances * sizeof(batch_instance), cudaMemcpyHostToDevice));
-  CHECK(cudaMemcpy(b.scratch + b.point_offset, point_offset.data(), (instances + 1) * 4, cudaMemcpyHostToDevice));
-  CHECK(cudaMemcpy(b.scratch + b.tile_seg, tile_seg.data(), tile_seg.size() * 4, cudaMemcpyHostToDevice));
-  for (const batch_group &g : b.groups)
-    CHECK(cudaMemcpy(b.scratch + g.members_dev, g.members.data(), g.members.size() * 4, cudaMemcpyHostToDevice));
-  CHECK(cudaMemset(b.scratch + b.io, 0, instances * sizeof(batch_io)));
-  // capture the chain
-  CHECK(cudaStreamCreateWithFlags(&b.capture, cudaStreamNonBlocking));
-  b.forks.resize(b.groups.size());
-  b.fork_events.resize(b.groups.size() + 1);
-  for (auto &fs : b.forks)
-    CHECK(cudaStreamCreateWithFlags(&fs, cudaStreamNonBlocking));
-  for (auto &e : b.fork_events)
-    CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-  CHECK(cudaStreamBeginCapture(b.capture, cudaStreamCaptureModeThreadLocal));
-  const cudaError_t enq = enqueue_batch(b);
-  cudaGraph_t graph = nullptr;
-  const cudaError_t end = cudaStreamEndCapture(b.capture, &graph);
-  b.graph = graph;
-  CHECK(enq);
-  CHECK(end);
-  CHECK(cudaGraphInstantiate(&b.exec, b.graph, 0));
-  *out = owner.release();
+  if (launches)
+    *launches = launched;
   return cudaSuccess;
 }
 
-cudaError_t batch_execute(batch_impl *b, const void *const *scalars, void *const *results, cudaStream_t stream) {
-  if (!b || !scalars || !results)
-    return cudaErrorInvalidValue;
-  int device = 0;
-  CHECK(cudaGetDevice(&device));
-  if (device != b->device)
-    return cudaErrorInvalidDevice;
-  for (unsigned k = 0; k < b->instances; k++)
-    if (!scalars[k] || !results[k] || (reinterpret_cast<uintptr_t>(scalars[k]) & 15) || (reinterpret_cast<uintptr_t>(results[k]) & 15))
-      return cudaErrorInvalidValue;
-  batch_io *io = b->at<batch_io>(b->io);
-  for (unsigned first = 0; first < b->instances; first += IO_CHUNK) {
+// Writes the instances' scalar and result pointers into the batch's io table.
+cudaError_t enqueue_io(batch_io *io, unsigned instances, const void *const *scalars, void *const *results, cudaStream_t stream) {
+  for (unsigned first = 0; first < instances; first += IO_CHUNK) {
     batch_io_update u{};
     u.first = first;
-    u.count = std::min(IO_CHUNK, b->instances - first);
+    u.count = std::min(IO_CHUNK, instances - first);
     for (unsigned k = 0; k < u.count; k++) {
       u.io[k].scalars = static_cast<const fe *>(scalars[first + k]);
       u.io[k].results = static_cast<jacobian *>(results[first + k]);
@@ -637,7 +549,96 @@ cudaError_t batch_execute(batch_impl *b, const void *const *scalars, void *const
     batch_set_io_kernel<<<1, IO_CHUNK, 0, stream>>>(io, u);
     CHECK(cudaGetLastError());
   }
-  return cudaGraphLaunch(b->exec, stream);
+  return cudaSuccess;
+}
+
+// A planned batch with its own scratch and captured graph.
+struct batch_impl {
+  int device = 0;
+  batch_plan b;
+  uint8_t *scratch = nullptr;
+  cudaStream_t capture = nullptr;
+  std::vector<cudaStream_t> forks;
+  std::vector<cudaEvent_t> fork_events;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  unsigned launches = 0;
+  ~batch_impl() {
+    if (exec)
+      cudaGraphExecDestroy(exec);
+    if (graph)
+      cudaGraphDestroy(graph);
+    for (cudaEvent_t e : fork_events)
+      cudaEventDestroy(e);
+    for (cudaStream_t s : forks)
+      cudaStreamDestroy(s);
+    if (capture)
+      cudaStreamDestroy(capture);
+    if (scratch)
+      cudaFree(scratch);
+  }
+};
+
+static cudaError_t device_sms(int device, int *sms) { return cudaDeviceGetAttribute(sms, cudaDevAttrMultiProcessorCount, device); }
+
+cudaError_t batch_create(batch_impl **out, const base_table_impl *table, const unsigned *counts, unsigned instances, const unsigned *window_bits) {
+  if (!out || !table)
+    return cudaErrorInvalidValue;
+  int device = 0, sms = 0;
+  CHECK(cudaGetDevice(&device));
+  if (device != table->device)
+    return cudaErrorInvalidDevice;
+  CHECK(device_sms(device, &sms));
+  std::unique_ptr<batch_impl> owner(new (std::nothrow) batch_impl);
+  if (!owner)
+    return cudaErrorMemoryAllocation;
+  batch_impl &bi = *owner;
+  bi.device = device;
+  CHECK(make_batch_plan(bi.b, table, counts, instances, window_bits, sms));
+  const batch_plan &b = bi.b;
+  CHECK(cudaMalloc(&bi.scratch, b.bytes));
+  const std::vector<uint8_t> img = descriptor_image(b);
+  CHECK(cudaMemcpy(bi.scratch + b.descriptors, img.data(), img.size(), cudaMemcpyHostToDevice));
+  CHECK(cudaMemset(bi.scratch + b.io, 0, instances * sizeof(batch_io)));
+  // capture the chain
+  CHECK(cudaStreamCreateWithFlags(&bi.capture, cudaStreamNonBlocking));
+  bi.forks.resize(b.groups.size());
+  bi.fork_events.resize(b.groups.size() + 1);
+  for (auto &fs : bi.forks)
+    CHECK(cudaStreamCreateWithFlags(&fs, cudaStreamNonBlocking));
+  for (auto &e : bi.fork_events)
+    CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  CHECK(cudaStreamBeginCapture(bi.capture, cudaStreamCaptureModeThreadLocal));
+  const cudaError_t enq = enqueue_batch(b, bi.scratch, bi.capture, bi.forks.data(), bi.fork_events.data(), &bi.launches);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t end = cudaStreamEndCapture(bi.capture, &graph);
+  bi.graph = graph;
+  CHECK(enq);
+  CHECK(end);
+  CHECK(cudaGraphInstantiate(&bi.exec, bi.graph, 0));
+  *out = owner.release();
+  return cudaSuccess;
+}
+
+static cudaError_t check_io(unsigned instances, const void *const *scalars, void *const *results) {
+  if (!scalars || !results)
+    return cudaErrorInvalidValue;
+  for (unsigned k = 0; k < instances; k++)
+    if (!scalars[k] || !results[k] || (reinterpret_cast<uintptr_t>(scalars[k]) & 15) || (reinterpret_cast<uintptr_t>(results[k]) & 15))
+      return cudaErrorInvalidValue;
+  return cudaSuccess;
+}
+
+cudaError_t batch_execute(batch_impl *bi, const void *const *scalars, void *const *results, cudaStream_t stream) {
+  if (!bi)
+    return cudaErrorInvalidValue;
+  int device = 0;
+  CHECK(cudaGetDevice(&device));
+  if (device != bi->device)
+    return cudaErrorInvalidDevice;
+  CHECK(check_io(bi->b.instances, scalars, results));
+  CHECK(enqueue_io(reinterpret_cast<batch_io *>(bi->scratch + bi->b.io), bi->b.instances, scalars, results, stream));
+  return cudaGraphLaunch(bi->exec, stream);
 }
 
 cudaError_t batch_set_up() {
@@ -703,11 +704,11 @@ bc_error msm_b200_batch_info(msm_b200_batch batch, size_t *scratch_bytes, unsign
     return bc_error_invalid_value;
   const msm_b200::batch_impl *b = reinterpret_cast<const msm_b200::batch_impl *>(batch);
   if (scratch_bytes)
-    *scratch_bytes = b->scratch_bytes;
+    *scratch_bytes = b->b.bytes;
   if (kernels)
     *kernels = b->launches;
   if (entries)
-    *entries = b->total_entries;
+    *entries = b->b.total_entries;
   return bc_success;
 }
 
