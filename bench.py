@@ -11,6 +11,19 @@ the device).  `value` times K steps with device-resident inputs (bases
 `e2e` times K steps through the same C ABI with the scalars in pinned host
 memory and the 254 results written to pinned host memory, copies included.
 
+Two more objects on the same line (rank 0, one GPU):
+  "batched"  the uneven 64-instance batch (lengths log-uniform in [2^10, 2^22],
+             seed 3, over one resident 2^22-point table): one execution of the
+             batched graph against 64 sequential plain calls; for the reference,
+             64 zero-padded msm_execute_async calls (--no-batched skips it);
+  "serving"  Poisson arrivals of requests with sizes log-uniform in [2^12, 2^23]
+             over a resident 2^23-point table and a 16 GiB scratch budget: the
+             request server (continuous batching) against a plain loop running
+             one request per call, p50/p99 latency and Mpoints/s at rates of 0.6,
+             0.9 and 1.2 times the plain loop's capacity (--serving-requests sets
+             the requests per rate, 200 by default, 10000 for the full config;
+             --no-serving skips it).
+
 --impl reference runs the reference era-bellman-cuda msm_execute_async built
 for sm_100a from its own sources (oracle/_ref/libbellman-cuda-ref.so) on the
 same inputs; that is the reference implementation of this path (a CUDA
@@ -51,6 +64,9 @@ def parse():
     ap.add_argument("--workload", choices=["uniform", "skewed"], default="uniform")
     ap.add_argument("--log-n", type=int, default=22)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the 64-instance batch")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving run")
+    ap.add_argument("--serving-requests", type=int, default=200, help="requests per rate (the full config: 10000)")
     return ap.parse_args()
 
 
@@ -194,6 +210,172 @@ def cpu_baseline(bc, scalars_all: np.ndarray, bases_dev: int, target_s: float = 
                       f"workload, {secs:.2f} s wall"}
 
 
+def generated_table(bc, seed: int, n: int, stream) -> int:
+    """n bases k_i * G (k_i from `seed`) generated on the device; returns the device pointer."""
+    import synth
+    kd = bc.to_device(synth.base_multipliers(seed, n))
+    bd = bc.malloc(n * 64)
+    bc.generator_multiples(kd, bd, n, stream)
+    bc.stream_synchronize(stream)
+    bc.free(kd)
+    return bd
+
+
+def batched_section(ours, bc, pool, stream, steps: int, warmup: int) -> dict:
+    """The uneven 64-instance batch (lengths log-uniform in [2^10, 2^22], seed 3;
+    even instances uniform, odd ones skewed; prefixes of one resident 2^22-point
+    table): one execution of the batched graph against 64 sequential plain calls
+    (for the reference: 64 calls padded with zero scalars to powers of two)."""
+    import synth
+    lengths = [int(x) for x in synth.batch_lengths(3, 64)]
+    n_table = 1 << 22
+    table_dev = generated_table(ours, 3, n_table, stream)
+    work = [s for _, s in synth.batch_workload(3, lengths)]
+    points = sum(lengths)
+    out = {"workload": "64 MSMs, lengths log-uniform in [2^10, 2^22] (seed 3), even instances uniform scalars, odd ones the skewed mix, "
+                       "prefixes of one resident 2^22-point base table", "instances": 64, "points": points}
+    if bc is ours:
+        table = bc.base_table_create(table_dev, n_table, stream)
+        sd = [bc.to_device(w) for w in work]
+        rd = [bc.malloc(254 * 96) for _ in lengths]
+        batch = bc.batch_create(table, lengths)
+        scratch, kernels, entries = bc.batch_info(batch)
+        for _ in range(warmup):
+            bc.batch_execute(batch, sd, rd, stream)
+        ms = time_steps(bc, stream, steps, lambda: bc.batch_execute(batch, sd, rd, stream))
+
+        def plain():
+            for n, s_, r in zip(lengths, sd, rd):
+                bc.check(bc.msm_any(pool, stream, table_dev, s_, r, n), "msm_b200_execute_async")
+
+        for _ in range(warmup):
+            plain()
+        ms_plain = time_steps(bc, stream, steps, plain)
+        out.update({"value": round(points / ms / 1e3, 2), "unit": "Mpoints/s", "ms": round(ms, 3),
+                    "plain_per_call": {"value": round(points / ms_plain / 1e3, 2), "ms": round(ms_plain, 3)},
+                    "speedup_vs_plain_per_call": round(ms_plain / ms, 3), "graph_kernels": kernels, "entries": entries,
+                    "scratch_gib": round(scratch / 2**30, 2), "table_gib": round(bc.base_table_bytes(table) / 2**30, 2)})
+        bc.batch_destroy(batch)
+        bc.base_table_destroy(table)
+        for p_ in sd + rd:
+            bc.free(p_)
+    else:  # the reference: one call per instance, zero-padded to the next power of two
+        bases = bc.to_device(ours.from_device(table_dev, (n_table, 16)))
+        padded = []
+        for w in work:
+            logn = max(0, (len(w) - 1).bit_length())
+            full = np.zeros((1 << logn, 8), np.uint32)
+            full[: len(w)] = w
+            padded.append((logn, bc.to_device(full)))
+        rd = bc.malloc(254 * 96)
+
+        def plain():
+            for logn, s_ in padded:
+                bc.msm(pool, stream, bases, s_, rd, logn)
+
+        for _ in range(warmup):
+            plain()
+        ms_plain = time_steps(bc, stream, steps, plain)
+        out.update({"plain_per_call": {"value": round(points / ms_plain / 1e3, 2), "ms": round(ms_plain, 3),
+                                       "note": "64 reference msm_execute_async calls, each zero-padded to a power of two"}})
+        for _, p_ in padded:
+            bc.free(p_)
+        bc.free(rd)
+        bc.free(bases)
+    ours.free(table_dev)
+    return out
+
+
+def serving_section(bc, pool, stream, requests: int, rates_rel=(0.6, 0.9, 1.2)) -> dict:
+    """Config 4 (reduced to `requests` requests unless asked for 10,000): Poisson
+    arrivals (seed 4), sizes log-uniform in [2^12, 2^23], scalars half uniform and
+    half skewed (device-resident slices of two 2^23-point pools), over a resident
+    2^23-point table with a 16 GiB scratch budget.  The server (continuous
+    batching) against a plain loop that runs one request per call in arrival
+    order; rates are multiples of the plain loop's measured capacity."""
+    import threading
+    import synth
+    n_table = 1 << 23
+    table_dev = generated_table(bc, 4, n_table, stream)
+    table = bc.base_table_create(table_dev, n_table, stream)
+    pools = {"uniform": bc.to_device(synth.uniform_scalars(40, n_table)), "skewed": bc.to_device(synth.skewed_scalars(41, n_table))}
+    rng = np.random.Generator(np.random.PCG64(np.random.SeedSequence([4, 5])))
+    sizes = np.rint(np.exp2(rng.uniform(12, 23, requests))).astype(np.int64)
+    offsets = [int(rng.integers(0, n_table - n + 1)) for n in sizes]
+    dists = ["uniform" if j % 2 == 0 else "skewed" for j in range(requests)]
+    src = [pools[d] + 32 * off for d, off in zip(dists, offsets)]
+    results = [bc.malloc(254 * 96) for _ in range(requests)]
+    points = int(sizes.sum())
+
+    # plain capacity: back-to-back calls, no arrivals
+    for j in range(min(8, requests)):
+        bc.msm_any(pool, stream, table_dev, src[j], results[j], int(sizes[j]))
+    bc.stream_synchronize(stream)
+    t0 = time.perf_counter()
+    for j in range(requests):
+        bc.msm_any(pool, stream, table_dev, src[j], results[j], int(sizes[j]))
+    bc.stream_synchronize(stream)
+    capacity = requests / (time.perf_counter() - t0)
+
+    def pct(lat):
+        return {"p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3)}
+
+    out = {"workload": f"{requests} requests, Poisson arrivals (seed 4), sizes log-uniform in [2^12, 2^23], half uniform / half skewed "
+                       "scalars, resident 2^23-point table, 16 GiB scratch budget",
+           "requests": requests, "points": points, "plain_capacity_rps": round(capacity, 1), "rates": []}
+    server = bc.server_create(table, 16 << 30, streams=4, max_group=16)
+    for rel in rates_rel:
+        rate = rel * capacity
+        gaps = np.random.Generator(np.random.PCG64(np.random.SeedSequence([4, int(rel * 1000)]))).exponential(1.0 / rate, requests)
+        # plain loop: one call per request, in arrival order
+        lat = np.zeros(requests)
+        start = time.perf_counter() + 0.01
+        arrival = start + np.cumsum(gaps)
+        for j in range(requests):
+            while time.perf_counter() < arrival[j]:
+                pass
+            bc.msm_any(pool, stream, table_dev, src[j], results[j], int(sizes[j]))
+            bc.stream_synchronize(stream)
+            lat[j] = (time.perf_counter() - arrival[j]) * 1e3
+        plain_span = time.perf_counter() - start
+        # server: a producer submits at the arrival times, this thread waits in order
+        tickets = [None] * requests
+        start = time.perf_counter() + 0.01
+        arrival = start + np.cumsum(gaps)
+
+        def producer():
+            for j in range(requests):
+                while time.perf_counter() < arrival[j]:
+                    pass
+                tickets[j] = bc.server_submit(server, src[j], int(sizes[j]), results[j])
+
+        th = threading.Thread(target=producer)
+        th.start()
+        th.join()
+        slat, first, last = np.zeros(requests), None, 0.0
+        groups = []
+        for j in range(requests):
+            rc, times = bc.server_wait(server, tickets[j])
+            bc.check(rc, "msm_b200_server_wait")
+            slat[j] = (times.done_us - times.submit_us) / 1e3
+            first = times.submit_us if first is None else min(first, times.submit_us)
+            last = max(last, times.done_us)
+            groups.append(times.group_size)
+        server_span = (last - first) / 1e6
+        out["rates"].append({"rate_rps": round(rate, 1), "rate_vs_plain_capacity": rel,
+                             "server": {"mpoints_s": round(points / server_span / 1e6, 2), **pct(slat), "mean_group": round(float(np.mean(groups)), 2)},
+                             "plain": {"mpoints_s": round(points / plain_span / 1e6, 2), **pct(lat)}})
+    stats = bc.server_stats(server)
+    out["server_groups"] = stats.groups
+    out["max_inflight_groups"] = stats.max_inflight_groups
+    bc.server_destroy(server)
+    for p_ in results + list(pools.values()):
+        bc.free(p_)
+    bc.base_table_destroy(table)
+    bc.free(table_dev)
+    return out
+
+
 def main():
     args = parse()
     dist = Dist(args.gpus)
@@ -333,6 +515,10 @@ def main():
                                 "bytes": "32 B scalar + 8 B/entry digit write; 20 B/entry per radix pass (4 histogram + 8 read + 8 write)"}
         if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(bc, scalars, bases_dev)
+    if dist.rank == 0 and dist.world == 1 and not args.no_batched:
+        line["batched"] = batched_section(ours, bc, pool, stream, max(3, args.steps // 2), 2)
+    if dist.rank == 0 and dist.world == 1 and not args.no_serving and args.impl == "b200":
+        line["serving"] = serving_section(bc, pool, stream, args.serving_requests)
     if dist.rank == 0:
         print(json.dumps(line))
     for p in (scalars_dev, results_dev, bases_dev):

@@ -104,6 +104,19 @@ class MsmB200Profile(ctypes.Structure):
         return self.nonzero_entries - self.nonempty_buckets - self.heads
 
 
+class RequestTimes(ctypes.Structure):
+    """msm_b200_request_times (include/bellman-cuda-b200.h)."""
+
+    _fields_ = [("submit_us", ctypes.c_double), ("start_us", ctypes.c_double), ("done_us", ctypes.c_double), ("group_size", ctypes.c_uint)]
+
+
+class ServerStats(ctypes.Structure):
+    """msm_b200_server_stats (include/bellman-cuda-b200.h)."""
+
+    _fields_ = [("groups", ctypes.c_ulonglong), ("requests", ctypes.c_ulonglong), ("max_inflight_groups", ctypes.c_ulonglong),
+                ("arena_bytes", ctypes.c_size_t), ("arena_used", ctypes.c_size_t), ("pending", ctypes.c_size_t)]
+
+
 def _ptr(x) -> Optional[int]:
     """numpy array -> host address; int -> as is; None -> NULL."""
     if x is None:
@@ -185,6 +198,11 @@ class BellmanCuda:
                 "msm_b200_batch_execute_async": [vp, ctypes.POINTER(vp), ctypes.POINTER(vp), Handle],
                 "msm_b200_batch_info": [vp, ctypes.POINTER(sz), ctypes.POINTER(u), ctypes.POINTER(ctypes.c_ulonglong)],
                 "msm_b200_batch_destroy": [vp],
+                "msm_b200_server_create": [ctypes.POINTER(vp), vp, sz, u, u],
+                "msm_b200_server_submit": [vp, vp, u, vp, ctypes.POINTER(ctypes.c_ulonglong)],
+                "msm_b200_server_wait": [vp, ctypes.c_ulonglong, ctypes.POINTER(RequestTimes)],
+                "msm_b200_server_get_stats": [vp, ctypes.POINTER(ServerStats)],
+                "msm_b200_server_destroy": [vp],
             }
             for name, args in ext.items():
                 f = getattr(L, name)
@@ -423,6 +441,31 @@ class BellmanCuda:
 
     def batch_destroy(self, batch: int) -> None:
         self.check(self.lib.msm_b200_batch_destroy(batch), "msm_b200_batch_destroy")
+
+    # -- request server ----------------------------------------------------------
+    def server_create(self, table: int, scratch_budget: int, streams: int = 4, max_group: int = 16) -> int:
+        h = ctypes.c_void_p()
+        self.check(self.lib.msm_b200_server_create(ctypes.byref(h), table, scratch_budget, streams, max_group), "msm_b200_server_create")
+        return h.value
+
+    def server_submit(self, server: int, scalars, count: int, results) -> int:
+        t = ctypes.c_ulonglong()
+        self.check(self.lib.msm_b200_server_submit(server, _ptr(scalars), count, _ptr(results), ctypes.byref(t)), "msm_b200_server_submit")
+        return t.value
+
+    def server_wait(self, server: int, ticket: int):
+        """(bc_error, RequestTimes) of one request; blocks until it has finished."""
+        times = RequestTimes()
+        rc = self.lib.msm_b200_server_wait(server, ticket, ctypes.byref(times))
+        return rc, times
+
+    def server_stats(self, server: int) -> ServerStats:
+        st = ServerStats()
+        self.check(self.lib.msm_b200_server_get_stats(server, ctypes.byref(st)), "msm_b200_server_get_stats")
+        return st
+
+    def server_destroy(self, server: int) -> None:
+        self.check(self.lib.msm_b200_server_destroy(server), "msm_b200_server_destroy")
 
     def default_window_bits(self, count: int) -> int:
         c = ctypes.c_uint()

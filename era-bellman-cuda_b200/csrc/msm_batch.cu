@@ -372,9 +372,6 @@ cudaError_t make_batch_plan(batch_plan &b, const base_table_impl *table, const u
     b.slots += (unsigned)g.members.size() << (g.c - 1);
     b.groups.push_back(g);
   }
-  b.tile_seg.resize(b.total_tiles);
-  for (unsigned k = 0; k < instances; k++)
-    std::fill(b.tile_seg.begin() + b.inst[k].tile_base, b.tile_seg.begin() + b.inst[k].tile_base + b.inst[k].tiles, k);
   const unsigned long long full = (unsigned long long)sms * ACC_MIN_BLOCKS * ACC_THREADS;
   b.acc_threads = (unsigned)std::max(1ull, std::min(full, (b.total_entries + 7) / 8));
   // scratch layout
@@ -420,7 +417,9 @@ std::vector<uint8_t> descriptor_image(const batch_plan &b) {
   auto put = [&](size_t off, const void *src, size_t bytes) { std::memcpy(img.data() + (off - b.descriptors), src, bytes); };
   put(b.inst_dev, b.inst.data(), b.instances * sizeof(batch_instance));
   put(b.point_offset_dev, b.point_offset.data(), (b.instances + 1) * 4);
-  put(b.tile_seg_dev, b.tile_seg.data(), b.tile_seg.size() * 4);
+  unsigned *tile_seg = reinterpret_cast<unsigned *>(img.data() + (b.tile_seg_dev - b.descriptors));
+  for (unsigned k = 0; k < b.instances; k++)
+    std::fill(tile_seg + b.inst[k].tile_base, tile_seg + b.inst[k].tile_base + b.inst[k].tiles, k);
   for (const batch_group &g : b.groups)
     put(g.members_dev, g.members.data(), g.members.size() * 4);
   return img;

@@ -59,7 +59,7 @@ struct batch_plan {
   unsigned long long total_entries = 0;
   unsigned total_points = 0, total_tiles = 0, slots = 0, sort_passes = 0, acc_threads = 0;
   std::vector<batch_instance> inst;
-  std::vector<unsigned> point_offset, tile_seg;
+  std::vector<unsigned> point_offset;
   std::vector<batch_group> groups;
   size_t keys[2], vals[2], counts, totals, zeros, buckets, flags, hb[2], hp[2], inst_dev, point_offset_dev, tile_seg_dev, io;
   size_t bytes = 0;       // scratch bytes

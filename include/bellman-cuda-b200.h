@@ -116,6 +116,45 @@ bc_error msm_b200_batch_execute_async(msm_b200_batch batch, const void *const *s
 bc_error msm_b200_batch_info(msm_b200_batch batch, size_t *scratch_bytes, unsigned *kernels, unsigned long long *entries);
 bc_error msm_b200_batch_destroy(msm_b200_batch batch);
 
+/* ---- Request server (no counterpart in the reference): continuous batching
+ * of MSM requests over one resident base table.
+ *
+ * Requests are submitted from any thread and queue in arrival order.  A
+ * scheduler thread admits them, oldest first, into groups that run as one
+ * batched kernel chain on one of `streams` device streams: a group grows
+ * while its scratch footprint fits in the largest free block of a device arena
+ * of `scratch_budget` bytes (allocated once, at creation) and it has at most
+ * `max_group` requests.  Groups admitted while others are still running
+ * overlap with them on the device; a finished group frees its arena block and
+ * stream, which admits the next requests.  A request longer than the table, or
+ * whose footprint exceeds the whole arena, finishes with an error. */
+typedef struct msm_b200_server_t *msm_b200_server;
+
+/* Host clock (microseconds since the server was created) of one request. */
+typedef struct msm_b200_request_times {
+  double submit_us, start_us, done_us; /* submitted, its group enqueued, its group finished */
+  unsigned group_size;                 /* requests in its group */
+} msm_b200_request_times;
+
+typedef struct msm_b200_server_stats {
+  unsigned long long groups, requests, max_inflight_groups;
+  size_t arena_bytes, arena_used, pending;
+} msm_b200_server_stats;
+
+bc_error msm_b200_server_create(msm_b200_server *server, msm_b200_base_table table, size_t scratch_budget, unsigned streams, unsigned max_group);
+/* Queues an MSM of `count` points over the first `count` points of the table.
+ * scalars: count Montgomery-form scalars; results: 254 Jacobian points (as
+ * msm_execute_async); each in device or host memory (host scalars are copied
+ * in when the request starts; pinned memory keeps the scheduler from
+ * blocking), valid until msm_b200_server_wait returns for the ticket. */
+bc_error msm_b200_server_submit(msm_b200_server server, const void *scalars, unsigned count, void *results, unsigned long long *ticket);
+/* Blocks until the request has finished; returns its status and (optional)
+ * its times, then forgets the ticket. */
+bc_error msm_b200_server_wait(msm_b200_server server, unsigned long long ticket, msm_b200_request_times *times);
+bc_error msm_b200_server_get_stats(msm_b200_server server, msm_b200_server_stats *stats);
+/* Finishes the queued requests, then releases the arena and streams. */
+bc_error msm_b200_server_destroy(msm_b200_server server);
+
 /* An MSM that allocates no memory (no counterpart in the reference).
  *
  * For callers that cannot allocate device memory at call time: code running
