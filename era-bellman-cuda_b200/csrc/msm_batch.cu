@@ -10,8 +10,8 @@
 // table).  All instances run as one kernel chain:
 //   digits       every point of every instance, W(c_k) signed digits each, into
 //                its instance's segment of W(c_k) * n_k (key, value) entries
-//   sort         segmented LSD radix sort, tile list over all segments
-//   zero counts  per segment
+//   sort         segmented LSD radix sort, tile list over all segments; the
+//                first pass drops zero digits (counted per segment)
 //   accumulate   the nonzero entries of all segments split into equal ranges,
 //                one per thread: the (instance, bucket-range) work list
 //   merge heads  as in the plain pipeline
@@ -58,7 +58,7 @@ static size_t align256(size_t v) { return (v + 255) & ~(size_t)255; }
 
 unsigned batch_window_bits(unsigned n) {
   const unsigned lg = ceil_log2_u(n);
-  for (const batch_tuning_row &row : BATCH_TUNING)
+  for (const tuning_row &row : BATCH_TUNING)
     if (lg <= row.max_log_n)
       return row.window_bits;
   return BATCH_TUNING[sizeof(BATCH_TUNING) / sizeof(BATCH_TUNING[0]) - 1].window_bits;
@@ -115,21 +115,27 @@ __global__ void __launch_bounds__(256) batch_digits_kernel(const batch_instance 
   const unsigned k = lo, i = g - s_off[k];
   const batch_instance d = inst[k];
   const fe *scalars = io[k].scalars;
-  scalar_digits(load_fe_streaming(scalars + i), d.c, d.windows, [&](unsigned w, uint32_t key, uint32_t negative) {
+  scalar_digits(load_fe_streaming(scalars + i), d.c, d.windows, [&](unsigned w, uint32_t magnitude, uint32_t negative) {
     const size_t out = d.entry_offset + (size_t)w * d.n + i;
-    keys[out] = key;
+    keys[out] = digit_key(magnitude);
     vals[out] = (w * d.stride + i) | (negative << 31);
   });
 }
 
+// The first pass drops zero digits (counted into zeros[k], which must start at
+// 0) and writes the nonzero entries of instance k to the end of its segment;
+// later passes sort that range only.
+template <bool FIRST>
 __global__ void __launch_bounds__(SORT_THREADS) batch_sort_histogram_kernel(const uint32_t *__restrict__ keys, const batch_instance *__restrict__ inst,
                                                                             const unsigned *__restrict__ tile_seg, unsigned shift,
-                                                                            uint32_t *__restrict__ counts) {
+                                                                            uint32_t *__restrict__ counts, uint32_t *__restrict__ zeros) {
   const unsigned t = blockIdx.x;
-  const batch_instance d = inst[tile_seg[t]];
+  const unsigned k = tile_seg[t];
+  const batch_instance d = inst[k];
+  const unsigned skip = FIRST ? 0 : zeros[k], live = d.entries - skip;
   const unsigned local = t - d.tile_base, base = local * SORT_TILE;
-  sort_histogram_tile(keys + d.entry_offset, base, min(SORT_TILE, d.entries - base), shift, counts + (size_t)d.tile_base * SORT_RADIX + local,
-                      d.tiles);
+  sort_histogram_tile<FIRST>(keys + d.entry_offset + skip, base, base < live ? min(SORT_TILE, live - base) : 0, shift,
+                             counts + (size_t)d.tile_base * SORT_RADIX + local, d.tiles, zeros + k);
 }
 
 // one warp per (segment, digit) row
@@ -143,35 +149,29 @@ __global__ void __launch_bounds__(256) batch_sort_scan_kernel(uint32_t *counts, 
 }
 
 template <bool STABLE>
-__global__ void __launch_bounds__(SORT_THREADS) batch_sort_scatter_kernel(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
+__global__ void __launch_bounds__(SORT_THREADS, STABLE ? 2 : 3) batch_sort_scatter_kernel(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
                                                                           uint32_t *__restrict__ keys_out, uint32_t *__restrict__ vals_out,
                                                                           const batch_instance *__restrict__ inst,
                                                                           const unsigned *__restrict__ tile_seg, unsigned shift,
-                                                                          const uint32_t *__restrict__ counts, const uint32_t *__restrict__ totals) {
+                                                                          const uint32_t *__restrict__ counts, const uint32_t *__restrict__ totals,
+                                                                          const uint32_t *__restrict__ zeros) {
   const unsigned t = blockIdx.x;
   const unsigned k = tile_seg[t];
   const batch_instance d = inst[k];
   const unsigned local = t - d.tile_base, base = local * SORT_TILE;
-  sort_scatter_tile<STABLE>(keys_in, vals_in, keys_out, vals_out, d.entry_offset, base, min(SORT_TILE, d.entries - base), shift,
-                            counts + (size_t)d.tile_base * SORT_RADIX + local, d.tiles, totals + (size_t)k * SORT_RADIX);
-}
-
-__global__ void batch_zero_counts_kernel(const uint32_t *__restrict__ keys, const batch_instance *__restrict__ inst, unsigned instances,
-                                         uint32_t *__restrict__ zeros) {
-  const unsigned k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= instances)
-    return;
-  const batch_instance d = inst[k];
-  const uint32_t *seg = keys + d.entry_offset;
-  unsigned lo = 0, hi = d.entries; // first index with key != 0
-  while (lo < hi) {
-    const unsigned mid = (lo + hi) >> 1;
-    if (seg[mid] == 0)
-      lo = mid + 1;
-    else
-      hi = mid;
+  const unsigned skip = zeros[k];
+  const uint32_t *tile_counts = counts + (size_t)d.tile_base * SORT_RADIX + local;
+  if (STABLE) {
+    const unsigned live = d.entries - skip;
+    if (base >= live)
+      return;
+    const size_t seg = d.entry_offset + skip;
+    sort_scatter_tile<true, false>(keys_in, vals_in, keys_out, vals_out, seg, seg, base, min(SORT_TILE, live - base), shift, tile_counts, d.tiles,
+                                   totals + (size_t)k * SORT_RADIX);
+  } else {
+    sort_scatter_tile<false, true>(keys_in, vals_in, keys_out, vals_out, d.entry_offset, d.entry_offset + skip, base,
+                                   min(SORT_TILE, d.entries - base), shift, tile_counts, d.tiles, totals + (size_t)k * SORT_RADIX);
   }
-  zeros[k] = lo;
 }
 
 // The batch's segments for accumulate_ranges: one per instance.
@@ -185,7 +185,7 @@ struct table_segments {
   __device__ __forceinline__ size_t first(unsigned s) const { return s_first[s]; }
   __device__ __forceinline__ size_t end(unsigned s) const { return s_end[s]; }
   __device__ __forceinline__ bool empty(unsigned s) const { return s_first[s] == s_end[s]; }
-  __device__ __forceinline__ unsigned bucket(unsigned s, uint32_t key) const { return s_bucket[s] + (key & s_mask[s]); }
+  __device__ __forceinline__ unsigned bucket(unsigned s, uint32_t key) const { return s_bucket[s] + key_slot(key, s_mask[s]); }
   __device__ __forceinline__ const affine *base(unsigned s, uint32_t val) const { return s_table[s] + (val & 0x7fffffffu); }
 };
 
@@ -359,7 +359,7 @@ cudaError_t make_batch_plan(batch_plan &b, const base_table_impl *table, const u
     return cudaErrorInvalidValue;
   b.point_offset[instances] = (unsigned)points;
   b.total_points = (unsigned)points;
-  b.sort_passes = (max_c + SORT_RADIX_BITS - 1) / SORT_RADIX_BITS;
+  b.sort_passes = (max_c - 1 + SORT_RADIX_BITS - 1) / SORT_RADIX_BITS; // keys take c - 1 bits
   for (auto &kv : by_c) {
     batch_group g;
     g.c = kv.first;
@@ -445,6 +445,7 @@ cudaError_t enqueue_batch(const batch_plan &b, uint8_t *scratch, cudaStream_t s,
   xyzz *hp[2] = {reinterpret_cast<xyzz *>(at(b.hp[0])), reinterpret_cast<xyzz *>(at(b.hp[1]))};
 
   CHECK(cudaMemsetAsync(flags, 0, b.slots, s));
+  CHECK(cudaMemsetAsync(zeros, 0, b.instances * sizeof(uint32_t), s));
   batch_digits_kernel<<<(b.total_points + 255) / 256, 256, 0, s>>>(inst, reinterpret_cast<const unsigned *>(at(b.point_offset_dev)), b.instances,
                                                                    b.total_points, io, keys[0], vals[0]);
   CHECK(cudaGetLastError());
@@ -453,26 +454,27 @@ cudaError_t enqueue_batch(const batch_plan &b, uint8_t *scratch, cudaStream_t s,
   const unsigned rows = b.instances * SORT_RADIX;
   for (unsigned pass = 0; pass < b.sort_passes; pass++) {
     const unsigned shift = pass * SORT_RADIX_BITS;
-    batch_sort_histogram_kernel<<<b.total_tiles, SORT_THREADS, 0, s>>>(keys[cur], inst, tile_seg, shift, counts);
+    if (pass == 0)
+      batch_sort_histogram_kernel<true><<<b.total_tiles, SORT_THREADS, 0, s>>>(keys[cur], inst, tile_seg, shift, counts, zeros);
+    else
+      batch_sort_histogram_kernel<false><<<b.total_tiles, SORT_THREADS, 0, s>>>(keys[cur], inst, tile_seg, shift, counts, zeros);
     CHECK(cudaGetLastError());
     batch_sort_scan_kernel<<<(rows * 32 + 255) / 256, 256, 0, s>>>(counts, inst, rows, totals);
     CHECK(cudaGetLastError());
     if (pass == 0)
       batch_sort_scatter_kernel<false><<<b.total_tiles, SORT_THREADS, 0, s>>>(keys[cur], vals[cur], keys[cur ^ 1], vals[cur ^ 1], inst, tile_seg,
-                                                                             shift, counts, totals);
+                                                                             shift, counts, totals, zeros);
     else
       batch_sort_scatter_kernel<true><<<b.total_tiles, SORT_THREADS, 0, s>>>(keys[cur], vals[cur], keys[cur ^ 1], vals[cur ^ 1], inst, tile_seg,
-                                                                            shift, counts, totals);
+                                                                            shift, counts, totals, zeros);
     CHECK(cudaGetLastError());
     launched += 3;
     cur ^= 1;
   }
-  batch_zero_counts_kernel<<<(b.instances + 127) / 128, 128, 0, s>>>(keys[cur], inst, b.instances, zeros);
-  CHECK(cudaGetLastError());
   batch_accumulate_kernel<<<(b.acc_threads + ACC_THREADS - 1) / ACC_THREADS, ACC_THREADS, 0, s>>>(
       keys[cur], vals[cur], inst, b.instances, zeros, b.acc_threads, buckets, flags, hb[0], hp[0]);
   CHECK(cudaGetLastError());
-  launched += 2;
+  launched++;
   unsigned heads = b.acc_threads;
   int h = 0;
   while (heads > 1) {

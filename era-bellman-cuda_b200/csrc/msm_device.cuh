@@ -107,6 +107,14 @@ template <class EMIT> __device__ __forceinline__ void scalar_digits(const fe &sc
   }
 }
 
+// Sort key of a signed digit of magnitude m = |d| in [0, 2^(c-1)]: m - 1, so
+// the keys of nonzero digits take c - 1 bits, and a zero digit wraps to
+// ZERO_KEY, which the first sort pass drops.  A key's bucket slot within its
+// window is m mod 2^(c-1): slot 0 holds m = 2^(c-1).
+constexpr uint32_t ZERO_KEY = 0xffffffffu;
+__host__ __device__ __forceinline__ uint32_t digit_key(uint32_t magnitude) { return magnitude - 1; }
+__host__ __device__ __forceinline__ uint32_t key_slot(uint32_t key, uint32_t slot_mask) { return (key + 1) & slot_mask; }
+
 // ---------------------------------------------------------------------------
 // LSD radix sort, tile level (one 8-bit digit per pass)
 // ---------------------------------------------------------------------------
@@ -117,25 +125,40 @@ __device__ __forceinline__ unsigned sort_digit(uint32_t key, unsigned shift) { r
 // Tile histogram of `count` keys at seg_keys[base..]: out[d * out_stride] =
 // number of keys whose current digit is d.  Per-warp shared counters (no
 // cross-warp contention); the dominant zero digit of sparse scalars is
-// counted with one ballot per warp.
+// counted with one ballot per warp.  DROP_ZEROS (the first pass): ZERO_KEY
+// entries (zero digits, which add nothing to any bucket) are left out of the
+// histogram and counted into *zero_count instead, so the scatter drops them.
+template <bool DROP_ZEROS>
 __device__ __forceinline__ void sort_histogram_tile(const uint32_t *__restrict__ seg_keys, unsigned base, unsigned count, unsigned shift,
-                                                    uint32_t *__restrict__ out, size_t out_stride) {
+                                                    uint32_t *__restrict__ out, size_t out_stride, uint32_t *__restrict__ zero_count) {
   __shared__ uint32_t hist[SORT_WARPS][SORT_RADIX];
+  __shared__ uint32_t s_zero_keys;
   const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (unsigned d = lane; d < SORT_RADIX; d += 32)
     hist[warp][d] = 0;
-  __syncwarp();
+  if (DROP_ZEROS && threadIdx.x == 0)
+    s_zero_keys = 0;
+  __syncthreads();
+  uint32_t zero_keys = 0;
 #pragma unroll 4
   for (unsigned k = 0; k < SORT_ITEMS; k++) {
     const unsigned i = k * SORT_THREADS + threadIdx.x;
-    const bool valid = i < count;
-    const unsigned d = valid ? sort_digit(seg_keys[base + i], shift) : 0;
+    bool valid = i < count;
+    const uint32_t key = valid ? seg_keys[base + i] : 0;
+    if (DROP_ZEROS) {
+      const unsigned dropped = __ballot_sync(0xffffffffu, valid && key == ZERO_KEY);
+      zero_keys += __popc(dropped);
+      valid = valid && key != ZERO_KEY;
+    }
+    const unsigned d = valid ? sort_digit(key, shift) : 0;
     const unsigned zeros = __ballot_sync(0xffffffffu, valid && d == 0);
     if (valid && d != 0)
       atomicAdd(&hist[warp][d], 1u);
     if (lane == 0 && zeros)
       hist[warp][0] += __popc(zeros);
   }
+  if (DROP_ZEROS && lane == 0 && zero_keys)
+    atomicAdd(&s_zero_keys, zero_keys);
   __syncthreads();
   for (unsigned d = threadIdx.x; d < SORT_RADIX; d += blockDim.x) {
     uint32_t sum = 0;
@@ -144,6 +167,8 @@ __device__ __forceinline__ void sort_histogram_tile(const uint32_t *__restrict__
       sum += hist[k][d];
     out[d * out_stride] = sum;
   }
+  if (DROP_ZEROS && threadIdx.x == 0 && s_zero_keys)
+    atomicAdd(zero_count, s_zero_keys);
 }
 
 // One warp: exclusive prefix of row[0..len) in place, the row total into
@@ -199,23 +224,26 @@ __device__ __forceinline__ void scan_256(const uint32_t *in, uint32_t *out, uint
   __syncthreads();
 }
 
-// Scatter one tile: `count` items at seg + base of a segment whose digit totals
-// are seg_totals[0..255]; tile_counts[d * count_stride] is this tile's exclusive
-// prefix over the segment's earlier tiles for digit d.  Ranks among equal digits: STABLE (every pass after the
+// Scatter one tile: `count` items at seg_in + base of a segment whose digit
+// totals are seg_totals[0..255], to seg_out + (digit base + rank);
+// tile_counts[d * count_stride] is this tile's exclusive prefix over the
+// segment's earlier tiles for digit d.  DROP_ZEROS (the first pass): ZERO_KEY
+// entries are not written (the histogram left them out).  Ranks among equal digits: STABLE (every pass after the
 // first, which LSD order requires) ranks warp by warp, 32 consecutive items
 // per round with __match_any_sync; the first pass may take any order and
 // ranks with shared atomics.  The tile is then reordered in shared memory so
 // that each digit's run is written to global memory with consecutive
 // addresses.
-template <bool STABLE>
+template <bool STABLE, bool DROP_ZEROS>
 __device__ __forceinline__ void sort_scatter_tile(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
-                                                  uint32_t *__restrict__ keys_out, uint32_t *__restrict__ vals_out, size_t seg, unsigned base,
-                                                  unsigned count, unsigned shift, const uint32_t *__restrict__ tile_counts, size_t count_stride,
-                                                  const uint32_t *__restrict__ seg_totals) {
+                                                  uint32_t *__restrict__ keys_out, uint32_t *__restrict__ vals_out, size_t seg_in, size_t seg_out,
+                                                  unsigned base, unsigned count, unsigned shift, const uint32_t *__restrict__ tile_counts,
+                                                  size_t count_stride, const uint32_t *__restrict__ seg_totals) {
   __shared__ uint32_t s_key[SORT_TILE];
   __shared__ uint32_t s_val[SORT_TILE];
   __shared__ uint32_t whist[STABLE ? SORT_WARPS : 1][SORT_RADIX];
   __shared__ uint32_t tile_cnt[SORT_RADIX], tile_off[SORT_RADIX], glob[SORT_RADIX], digit_base[SORT_RADIX], warp_sums[SORT_WARPS];
+  __shared__ uint32_t staged;
   const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const unsigned sub = warp * (32 * SORT_ITEMS); // this warp's items: base + sub + r*32 + lane
   if (STABLE) {
@@ -231,9 +259,10 @@ __device__ __forceinline__ void sort_scatter_tile(const uint32_t *__restrict__ k
 #pragma unroll
   for (unsigned r = 0; r < SORT_ITEMS; r++) {
     const unsigned i = sub + r * 32 + lane;
-    const bool valid = i < count;
-    key[r] = valid ? keys_in[seg + base + i] : 0;
-    val[r] = valid ? vals_in[seg + base + i] : 0;
+    const bool in_tile = i < count;
+    key[r] = in_tile ? keys_in[seg_in + base + i] : 0;
+    val[r] = in_tile ? vals_in[seg_in + base + i] : 0;
+    const bool valid = in_tile && (!DROP_ZEROS || key[r] != ZERO_KEY);
     const unsigned d = valid ? sort_digit(key[r], shift) : SORT_RADIX;
     if (STABLE) {
       const unsigned peers = __match_any_sync(0xffffffffu, d);
@@ -263,6 +292,8 @@ __device__ __forceinline__ void sort_scatter_tile(const uint32_t *__restrict__ k
     __syncthreads();
   }
   scan_256(tile_cnt, tile_off, warp_sums);
+  if (threadIdx.x == SORT_RADIX - 1)
+    staged = tile_off[SORT_RADIX - 1] + tile_cnt[SORT_RADIX - 1]; // items kept (dropped zero keys excluded)
   for (unsigned d = threadIdx.x; d < SORT_RADIX; d += blockDim.x)
     glob[d] = seg_totals[d];
   __syncthreads();
@@ -272,7 +303,7 @@ __device__ __forceinline__ void sort_scatter_tile(const uint32_t *__restrict__ k
 #pragma unroll
   for (unsigned r = 0; r < SORT_ITEMS; r++) {
     const unsigned i = sub + r * 32 + lane;
-    if (i < count) {
+    if (i < count && (!DROP_ZEROS || key[r] != ZERO_KEY)) {
       const unsigned d = sort_digit(key[r], shift);
       const unsigned pos = tile_off[d] + (STABLE ? whist[warp][d] : 0) + rank[r];
       s_key[pos] = key[r];
@@ -283,10 +314,10 @@ __device__ __forceinline__ void sort_scatter_tile(const uint32_t *__restrict__ k
 #pragma unroll 4
   for (unsigned j = 0; j < SORT_ITEMS; j++) {
     const unsigned pos = j * SORT_THREADS + threadIdx.x;
-    if (pos < count) {
+    if (pos < staged) {
       const uint32_t k = s_key[pos];
       const unsigned d = sort_digit(k, shift);
-      const size_t out = seg + glob[d] + (pos - tile_off[d]);
+      const size_t out = seg_out + glob[d] + (pos - tile_off[d]);
       keys_out[out] = k;
       vals_out[out] = s_val[pos];
     }

@@ -9,6 +9,7 @@
 #include "bellman-cuda-b200.h"
 #include "msm_host.cuh"
 #include "msm_kernels.cuh"
+#include "plain_tuning.h"
 
 #include <algorithm>
 #include <cstdlib>
@@ -33,16 +34,15 @@ static unsigned ceil_log2(unsigned long long v) {
   return r;
 }
 
-// Window width by problem size: Pippenger cost ~ (n + 1.4 * 2^c) / c point
-// additions, minimised near c = log2(n) - 3 .. - 6 at the sizes of interest;
-// capped at 16 so keys need at most two 8-bit sort passes.
+// Window width by problem size: the checked-in table measured by the
+// autotuner (era-bellman-cuda_b200/autotune.py --plain).  Keys take c - 1
+// bits, so every width up to 17 sorts in two 8-bit passes.
 unsigned default_window_bits(unsigned long long n) {
   const unsigned lg = ceil_log2(n);
-  if (lg <= 6)
-    return 3;
-  if (lg <= 20)
-    return std::max(3u, lg - 4);
-  return 16;
+  for (const tuning_row &row : PLAIN_TUNING)
+    if (lg <= row.max_log_n)
+      return row.window_bits;
+  return PLAIN_TUNING[sizeof(PLAIN_TUNING) / sizeof(PLAIN_TUNING[0]) - 1].window_bits;
 }
 
 struct device_info {
@@ -70,7 +70,7 @@ plan make_plan(unsigned n, unsigned window_bits, int sms) {
   p.c = window_bits ? window_bits : default_window_bits(n);
   p.windows = (RESULT_BITS + p.c - 1) / p.c;
   p.log_b = p.c - 1;
-  p.key_bits = p.c; // keys are |d| in [0, 2^(c-1)]
+  p.key_bits = p.c - 1; // keys are |d| - 1 for |d| in [1, 2^(c-1)]
   p.sort_passes = (p.key_bits + SORT_RADIX_BITS - 1) / SORT_RADIX_BITS;
   p.tiles = (n + SORT_TILE - 1) / SORT_TILE;
   // One accumulation range per resident thread (4 blocks of ACC_THREADS per
@@ -233,10 +233,11 @@ static cudaError_t enqueue_accumulation(const plan &p, const fe *scalars, const 
   const unsigned n = p.n;
 
   // 1. digits (with the first sort pass's histograms when they fit in shared memory)
+  CHECK(cudaMemsetAsync(zeros, 0, p.windows * sizeof(uint32_t), stream));
   const bool fused_histogram = p.windows <= MAX_FUSED_HISTOGRAM_WINDOWS;
   if (fused_histogram) {
-    digits_histogram_kernel<<<p.tiles, SORT_THREADS, p.windows * SORT_RADIX * 4, stream>>>(scalars, n, p.c, p.windows, p.tiles, keys[0],
-                                                                                            vals[0], counts);
+    digits_histogram_kernel<<<p.tiles, SORT_THREADS, p.windows * (SORT_RADIX + 1) * 4, stream>>>(scalars, n, p.c, p.windows, p.tiles, keys[0],
+                                                                                                  vals[0], counts, zeros);
   } else {
     digits_kernel<<<(n + 255) / 256, 256, 0, stream>>>(scalars, n, p.c, p.windows, keys[0], vals[0]);
   }
@@ -251,7 +252,10 @@ static cudaError_t enqueue_accumulation(const plan &p, const fe *scalars, const 
     const unsigned shift = pass * SORT_RADIX_BITS;
     const dim3 grid(p.tiles, p.windows);
     if (pass > 0 || !fused_histogram) {
-      sort_histogram_kernel<<<grid, SORT_THREADS, 0, stream>>>(keys[cur], n, p.tiles, shift, counts);
+      if (pass == 0)
+        sort_histogram_first_kernel<<<grid, SORT_THREADS, 0, stream>>>(keys[cur], n, p.tiles, shift, counts, zeros);
+      else
+        sort_histogram_kernel<<<grid, SORT_THREADS, 0, stream>>>(keys[cur], n, p.tiles, shift, counts, zeros);
       CHECK(cudaGetLastError());
       m.launched++;
     }
@@ -259,20 +263,17 @@ static cudaError_t enqueue_accumulation(const plan &p, const fe *scalars, const 
     CHECK(cudaGetLastError());
     if (pass == 0)
       sort_scatter_first_kernel<<<grid, SORT_THREADS, 0, stream>>>(keys[cur], vals[cur], keys[cur ^ 1], vals[cur ^ 1], n, p.tiles, shift, counts,
-                                                                   totals);
+                                                                   totals, zeros);
     else
       sort_scatter_stable_kernel<<<grid, SORT_THREADS, 0, stream>>>(keys[cur], vals[cur], keys[cur ^ 1], vals[cur ^ 1], n, p.tiles, shift, counts,
-                                                                    totals);
+                                                                    totals, zeros);
     CHECK(cudaGetLastError());
     m.launched += 2;
     cur ^= 1;
   }
   CHECK(m.mark(stream));
 
-  // 3. zero-digit prefix of every window
-  zero_counts_kernel<<<(p.windows + 127) / 128, 128, 0, stream>>>(keys[cur], n, p.windows, zeros);
-  CHECK(cudaGetLastError());
-  m.launched++;
+  // 3. zero digits: counted by the first sort pass (the stage is empty)
   CHECK(m.mark(stream));
 
   // 4. accumulation
@@ -579,7 +580,7 @@ template <class F> static cudaError_t set_carveout(F *func, int percent) {
 
 cudaError_t set_up() {
   CHECK(cudaFuncSetAttribute(digits_histogram_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             MAX_FUSED_HISTOGRAM_WINDOWS * SORT_RADIX * 4));
+                             MAX_FUSED_HISTOGRAM_WINDOWS * (SORT_RADIX + 1) * 4));
   CHECK(set_carveout(accumulate_kernel, ACC_CARVEOUT)); // 4 blocks x 18 KB of base-point slots
   CHECK(set_carveout(merge_heads_kernel, cudaSharedmemCarveoutMaxL1));
   CHECK(set_carveout(reduce_groups_kernel, cudaSharedmemCarveoutMaxL1));

@@ -9,38 +9,43 @@ __global__ void __launch_bounds__(256) digits_kernel(const fe *__restrict__ scal
   const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n)
     return;
-  scalar_digits(load_fe_streaming(scalars + i), c, windows, [&](unsigned w, uint32_t key, uint32_t negative) {
+  scalar_digits(load_fe_streaming(scalars + i), c, windows, [&](unsigned w, uint32_t magnitude, uint32_t negative) {
     const size_t out = (size_t)w * n + i;
-    keys[out] = key;
+    keys[out] = digit_key(magnitude);
     vals[out] = i | (negative << 31);
   });
 }
 
 // The same, one block per sort tile (SORT_TILE scalars), also producing the
-// first radix pass's tile histograms (low 8 bits of every window's keys), so
-// that pass needs no histogram kernel.  Dynamic shared memory: windows x 256
-// counters.
+// first radix pass's tile histograms (low 8 bits of every window's nonzero
+// keys), so that pass needs no histogram kernel, and adding each window's
+// zero digits to zeros[w].  Dynamic shared memory: windows x 257 counters.
 __global__ void __launch_bounds__(SORT_THREADS) digits_histogram_kernel(const fe *__restrict__ scalars, unsigned n, unsigned c, unsigned windows,
                                                                         unsigned tiles, uint32_t *__restrict__ keys, uint32_t *__restrict__ vals,
-                                                                        uint32_t *__restrict__ counts) {
-  extern __shared__ uint32_t hist[]; // [windows][SORT_RADIX]
+                                                                        uint32_t *__restrict__ counts, uint32_t *__restrict__ zeros) {
+  extern __shared__ uint32_t hist[]; // [windows][SORT_RADIX], then [windows] zero digits
+  uint32_t *zero_digits = hist + windows * SORT_RADIX;
   const unsigned tile = blockIdx.x;
-  for (unsigned k = threadIdx.x; k < windows * SORT_RADIX; k += blockDim.x)
+  for (unsigned k = threadIdx.x; k < windows * (SORT_RADIX + 1); k += blockDim.x)
     hist[k] = 0;
   __syncthreads();
   for (unsigned k = 0; k < SORT_ITEMS; k++) {
     const unsigned i = tile * SORT_TILE + k * SORT_THREADS + threadIdx.x;
     if (i < n)
-      scalar_digits(load_fe_streaming(scalars + i), c, windows, [&](unsigned w, uint32_t key, uint32_t negative) {
+      scalar_digits(load_fe_streaming(scalars + i), c, windows, [&](unsigned w, uint32_t magnitude, uint32_t negative) {
         const size_t out = (size_t)w * n + i;
+        const uint32_t key = digit_key(magnitude);
         keys[out] = key;
         vals[out] = i | (negative << 31);
-        atomicAdd(&hist[w * SORT_RADIX + (key & (SORT_RADIX - 1))], 1u);
+        atomicAdd(magnitude ? &hist[w * SORT_RADIX + (key & (SORT_RADIX - 1))] : &zero_digits[w], 1u);
       });
   }
   __syncthreads();
   for (unsigned k = threadIdx.x; k < windows * SORT_RADIX; k += blockDim.x)
     counts[(size_t)k * tiles + tile] = hist[k]; // k = w * 256 + d
+  for (unsigned w = threadIdx.x; w < windows; w += blockDim.x)
+    if (zero_digits[w])
+      atomicAdd(&zeros[w], zero_digits[w]);
 }
 
 // ---------------------------------------------------------------------------
@@ -49,12 +54,30 @@ __global__ void __launch_bounds__(SORT_THREADS) digits_histogram_kernel(const fe
 //    per (window, digit), the exclusive prefix over tiles, and digit_base
 //    [window][digit] the exclusive prefix over digits: an element's output
 //    position is digit_base + counts + its rank among equal digits in the tile.
+//    The first pass drops zero digits (they add nothing to any bucket): it
+//    counts them into zeros[w] and writes the nonzero entries of window w to
+//    [w n + zeros[w], (w + 1) n); later passes sort that range only (tiles
+//    past its end have nothing to do).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(SORT_THREADS) sort_histogram_kernel(const uint32_t *__restrict__ keys, unsigned n, unsigned tiles,
-                                                                      unsigned shift, uint32_t *__restrict__ counts) {
+template <bool FIRST>
+__device__ __forceinline__ void sort_histogram_window(const uint32_t *__restrict__ keys, unsigned n, unsigned tiles, unsigned shift,
+                                                      uint32_t *__restrict__ counts, uint32_t *__restrict__ zeros) {
   const unsigned tile = blockIdx.x, w = blockIdx.y;
+  const unsigned skip = FIRST ? 0 : zeros[w], live = n - skip;
   const unsigned base = tile * SORT_TILE;
-  sort_histogram_tile(keys + (size_t)w * n, base, min(SORT_TILE, n - base), shift, counts + (size_t)w * SORT_RADIX * tiles + tile, tiles);
+  sort_histogram_tile<FIRST>(keys + (size_t)w * n + skip, base, base < live ? min(SORT_TILE, live - base) : 0, shift,
+                             counts + (size_t)w * SORT_RADIX * tiles + tile, tiles, zeros + w);
+}
+
+__global__ void __launch_bounds__(SORT_THREADS) sort_histogram_first_kernel(const uint32_t *__restrict__ keys, unsigned n, unsigned tiles,
+                                                                            unsigned shift, uint32_t *__restrict__ counts,
+                                                                            uint32_t *__restrict__ zeros) {
+  sort_histogram_window<true>(keys, n, tiles, shift, counts, zeros);
+}
+
+__global__ void __launch_bounds__(SORT_THREADS) sort_histogram_kernel(const uint32_t *__restrict__ keys, unsigned n, unsigned tiles, unsigned shift,
+                                                                      uint32_t *__restrict__ counts, const uint32_t *__restrict__ zeros) {
+  sort_histogram_window<false>(keys, n, tiles, shift, counts, const_cast<uint32_t *>(zeros));
 }
 
 // One warp per (window, digit) row of counts (see sort_scan_row).
@@ -65,45 +88,31 @@ __global__ void __launch_bounds__(256) sort_scan_kernel(uint32_t *counts, unsign
   sort_scan_row(counts + (size_t)row * tiles, tiles, totals + row);
 }
 
-__global__ void __launch_bounds__(SORT_THREADS) sort_scatter_first_kernel(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
+__global__ void __launch_bounds__(SORT_THREADS, 3) sort_scatter_first_kernel(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
                                                                           uint32_t *__restrict__ keys_out, uint32_t *__restrict__ vals_out,
                                                                           unsigned n, unsigned tiles, unsigned shift,
-                                                                          const uint32_t *__restrict__ counts,
-                                                                          const uint32_t *__restrict__ totals) {
+                                                                          const uint32_t *__restrict__ counts, const uint32_t *__restrict__ totals,
+                                                                          const uint32_t *__restrict__ zeros) {
   const unsigned tile = blockIdx.x, w = blockIdx.y;
   const unsigned base = tile * SORT_TILE;
-  sort_scatter_tile<false>(keys_in, vals_in, keys_out, vals_out, (size_t)w * n, base, min(SORT_TILE, n - base), shift,
-                           counts + (size_t)w * SORT_RADIX * tiles + tile, tiles, totals + (size_t)w * SORT_RADIX);
+  const size_t seg = (size_t)w * n;
+  sort_scatter_tile<false, true>(keys_in, vals_in, keys_out, vals_out, seg, seg + zeros[w], base, min(SORT_TILE, n - base), shift,
+                                 counts + (size_t)w * SORT_RADIX * tiles + tile, tiles, totals + (size_t)w * SORT_RADIX);
 }
 
 __global__ void __launch_bounds__(SORT_THREADS) sort_scatter_stable_kernel(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
                                                                            uint32_t *__restrict__ keys_out, uint32_t *__restrict__ vals_out,
                                                                            unsigned n, unsigned tiles, unsigned shift,
-                                                                           const uint32_t *__restrict__ counts,
-                                                                           const uint32_t *__restrict__ totals) {
+                                                                           const uint32_t *__restrict__ counts, const uint32_t *__restrict__ totals,
+                                                                           const uint32_t *__restrict__ zeros) {
   const unsigned tile = blockIdx.x, w = blockIdx.y;
+  const unsigned skip = zeros[w], live = n - skip;
   const unsigned base = tile * SORT_TILE;
-  sort_scatter_tile<true>(keys_in, vals_in, keys_out, vals_out, (size_t)w * n, base, min(SORT_TILE, n - base), shift,
-                          counts + (size_t)w * SORT_RADIX * tiles + tile, tiles, totals + (size_t)w * SORT_RADIX);
-}
-
-// ---------------------------------------------------------------------------
-// 3. first nonzero key of each sorted window
-// ---------------------------------------------------------------------------
-__global__ void zero_counts_kernel(const uint32_t *__restrict__ keys, unsigned n, unsigned windows, uint32_t *__restrict__ zeros) {
-  const unsigned w = blockIdx.x * blockDim.x + threadIdx.x;
-  if (w >= windows)
+  if (base >= live)
     return;
-  const uint32_t *seg = keys + (size_t)w * n;
-  unsigned lo = 0, hi = n; // first index with key != 0
-  while (lo < hi) {
-    const unsigned mid = (lo + hi) >> 1;
-    if (seg[mid] == 0)
-      lo = mid + 1;
-    else
-      hi = mid;
-  }
-  zeros[w] = lo;
+  const size_t seg = (size_t)w * n + skip;
+  sort_scatter_tile<true, false>(keys_in, vals_in, keys_out, vals_out, seg, seg, base, min(SORT_TILE, live - base), shift,
+                                 counts + (size_t)w * SORT_RADIX * tiles + tile, tiles, totals + (size_t)w * SORT_RADIX);
 }
 
 // ---------------------------------------------------------------------------
@@ -112,7 +121,7 @@ __global__ void zero_counts_kernel(const uint32_t *__restrict__ keys, unsigned n
 constexpr unsigned MAX_WINDOWS = 128;
 
 // The plain pipeline's segments: window w holds entries [w n, (w + 1) n), its
-// zero digits first; bucket slot of a key = (w << log_b) | (key & mask).
+// nonzero entries last; bucket slot of a key = (w << log_b) | key_slot(key).
 struct window_segments {
   const affine *__restrict__ bases;
   const uint32_t *s_zeros;            // shared: zero-digit prefix per window
@@ -123,7 +132,7 @@ struct window_segments {
   __device__ __forceinline__ size_t first(unsigned w) const { return (size_t)w * n + s_zeros[w]; }
   __device__ __forceinline__ size_t end(unsigned w) const { return (size_t)(w + 1) * n; }
   __device__ __forceinline__ bool empty(unsigned w) const { return s_zeros[w] == n; }
-  __device__ __forceinline__ unsigned bucket(unsigned w, uint32_t key) const { return (w << log_b) | (key & ((1u << log_b) - 1)); }
+  __device__ __forceinline__ unsigned bucket(unsigned w, uint32_t key) const { return (w << log_b) | key_slot(key, (1u << log_b) - 1); }
   __device__ __forceinline__ const affine *base(unsigned, uint32_t val) const { return bases + (val & 0x7fffffffu); }
 };
 

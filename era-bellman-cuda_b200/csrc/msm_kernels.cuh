@@ -3,9 +3,11 @@
 // Pipeline for n points, window width c, W = ceil(254 / c) windows and
 // B = 2^(c-1) bucket slots per window:
 //   1. digits      scalars -> signed c-bit digits of min(s, r - s); per window
-//                  a key |d| in [0, B] and a value (point index | sign << 31)
-//   2. sort        LSD radix sort of (key, value) inside each window segment
-//   3. zero_counts first nonzero key of every window (zero digits sort first)
+//                  a key |d| - 1 (c - 1 bits; a zero digit wraps to ZERO_KEY)
+//                  and a value (point index | sign << 31)
+//   2. sort        LSD radix sort of (key, value) inside each window segment;
+//                  the first pass drops zero digits (counted per window), so
+//                  window w keeps its nonzero entries at the end of its segment
 //   4. accumulate  the nonzero entries of all windows are split into equal
 //                  contiguous ranges, one per thread; each thread adds its
 //                  range bucket by bucket (XYZZ += affine); buckets that start
@@ -50,7 +52,7 @@ struct plan {
   unsigned c;           // window bits
   unsigned windows;     // W
   unsigned log_b;       // log2 of bucket slots per window (c - 1)
-  unsigned key_bits;    // bits of a key (keys are in [0, 2^log_b])
+  unsigned key_bits;    // bits of a sort key (|d| - 1 for |d| in [1, 2^log_b])
   unsigned sort_passes; // radix passes
   unsigned tiles;       // sort tiles per window
   unsigned acc_threads; // accumulation threads (ranges)
@@ -70,28 +72,30 @@ struct plan {
 // and the top window of a W*c >= 254 split never carries out.
 __global__ void digits_kernel(const fe *__restrict__ scalars, unsigned n, unsigned c, unsigned windows, uint32_t *__restrict__ keys,
                               uint32_t *__restrict__ vals);
-// the same, also writing the first radix pass's tile histograms
+// the same, also writing the first radix pass's tile histograms of the
+// nonzero keys and adding each window's zero digits to zeros[w]
 __global__ void digits_histogram_kernel(const fe *__restrict__ scalars, unsigned n, unsigned c, unsigned windows, unsigned tiles,
-                                        uint32_t *__restrict__ keys, uint32_t *__restrict__ vals, uint32_t *__restrict__ counts);
+                                        uint32_t *__restrict__ keys, uint32_t *__restrict__ vals, uint32_t *__restrict__ counts,
+                                        uint32_t *__restrict__ zeros);
 
 // ---------------------------------------------------------------------------
-// 2. sort (keys and values per window segment of n entries)
+// 2. sort (keys and values per window segment of n entries); the first pass
+//    drops zero digits, counting them in zeros[w] (which must start at 0)
 // ---------------------------------------------------------------------------
-__global__ void sort_histogram_kernel(const uint32_t *__restrict__ keys, unsigned n, unsigned tiles, unsigned shift,
-                                      uint32_t *__restrict__ counts);
+__global__ void sort_histogram_first_kernel(const uint32_t *__restrict__ keys, unsigned n, unsigned tiles, unsigned shift,
+                                            uint32_t *__restrict__ counts, uint32_t *__restrict__ zeros);
+__global__ void sort_histogram_kernel(const uint32_t *__restrict__ keys, unsigned n, unsigned tiles, unsigned shift, uint32_t *__restrict__ counts,
+                                      const uint32_t *__restrict__ zeros);
 __global__ void sort_scan_kernel(uint32_t *counts, unsigned tiles, unsigned rows, uint32_t *__restrict__ totals);
 // first pass (any order among equal digits) and later passes (stable)
 __global__ void sort_scatter_first_kernel(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in, uint32_t *__restrict__ keys_out,
                                           uint32_t *__restrict__ vals_out, unsigned n, unsigned tiles, unsigned shift,
-                                          const uint32_t *__restrict__ counts, const uint32_t *__restrict__ totals);
+                                          const uint32_t *__restrict__ counts, const uint32_t *__restrict__ totals,
+                                          const uint32_t *__restrict__ zeros);
 __global__ void sort_scatter_stable_kernel(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in, uint32_t *__restrict__ keys_out,
                                            uint32_t *__restrict__ vals_out, unsigned n, unsigned tiles, unsigned shift,
-                                           const uint32_t *__restrict__ counts, const uint32_t *__restrict__ totals);
-
-// ---------------------------------------------------------------------------
-// 3. zero counts
-// ---------------------------------------------------------------------------
-__global__ void zero_counts_kernel(const uint32_t *__restrict__ keys, unsigned n, unsigned windows, uint32_t *__restrict__ zeros);
+                                           const uint32_t *__restrict__ counts, const uint32_t *__restrict__ totals,
+                                           const uint32_t *__restrict__ zeros);
 
 // ---------------------------------------------------------------------------
 // 4. accumulation

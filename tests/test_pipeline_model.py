@@ -9,6 +9,11 @@ import random
 import pytest
 
 R = 0x30644E72E131A029B85045B68181585D2833E84879B9709143E1F593F0000001
+ZERO_KEY = 0xFFFFFFFF  # sort key of a zero digit (|d| - 1 wrapped)
+
+
+def key_slot(key, B):
+    return (key + 1) & (B - 1)
 
 
 def model_msm(scal, kl, c, T, chunk=4, log_m_max=4):
@@ -32,13 +37,15 @@ def model_msm(scal, kl, c, T, chunk=4, log_m_max=4):
                 raw, negd, carry = (1 << c) - raw, 1, 1
             else:
                 carry = 0
-            keys[w][i], vals[w][i] = raw, (i, negd ^ flip)
+            keys[w][i], vals[w][i] = (raw - 1) & 0xFFFFFFFF, (i, negd ^ flip)
         assert carry == 0
+    # the first sort pass drops zero digits; the nonzero entries of a window
+    # end up sorted at the end of its segment (the prefix is never read)
     for w in range(W):
-        order = sorted(range(n), key=lambda i: keys[w][i])
+        order = sorted(range(n), key=lambda i: (keys[w][i] != ZERO_KEY, keys[w][i]))
         keys[w] = [keys[w][i] for i in order]
         vals[w] = [vals[w][i] for i in order]
-    zeros = [sum(1 for k in keys[w] if k == 0) for w in range(W)]
+    zeros = [sum(1 for k in keys[w] if k == ZERO_KEY) for w in range(W)]
     pre = [0]
     for w in range(W):
         pre.append(pre[-1] + n - zeros[w])
@@ -60,10 +67,10 @@ def model_msm(scal, kl, c, T, chunk=4, log_m_max=4):
         w, idx = entry(beg)
         key = keys[w][idx]
         cont = idx > zeros[w] and keys[w][idx - 1] == key
-        cur, acc, first = (w << log_b) | (key & (B - 1)), point(w, idx), True
+        cur, acc, first = (w << log_b) | key_slot(key, B), point(w, idx), True
         for v in range(beg + 1, end):
             w, idx = entry(v)
-            b = (w << log_b) | (keys[w][idx] & (B - 1))
+            b = (w << log_b) | key_slot(keys[w][idx], B)
             if b != cur:
                 if first and cont:
                     hb[t], hp[t] = cur, acc
