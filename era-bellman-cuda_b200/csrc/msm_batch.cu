@@ -502,26 +502,15 @@ cudaError_t enqueue_batch(const batch_plan &b, uint8_t *scratch, cudaStream_t s,
                                                                                                    streams[0]);
     CHECK(cudaGetLastError());
     launched++;
-    int t = 0;
     for (unsigned level = 0; level < p.log_g; level++) {
-      const unsigned threads = p.windows * ((1u << p.log_g) >> (level + 1));
-      reduce_tree_kernel<<<(threads + ACC_THREADS - 1) / ACC_THREADS, ACC_THREADS, 0, fs>>>(tree[t], tree[t ^ 1], streams[0], p.windows, p.log_g,
-                                                                                             level);
+      const unsigned threads = p.windows * (level + 2) * ((1u << p.log_g) >> (level + 1));
+      const int in = level & 1;
+      reduce_level_kernel<<<(threads + ACC_THREADS - 1) / ACC_THREADS, ACC_THREADS, 0, fs>>>(tree[in], tree[in ^ 1], streams[in], streams[in ^ 1],
+                                                                                              p.windows, p.log_g, level);
       CHECK(cudaGetLastError());
       launched++;
-      t ^= 1;
     }
-    int si = 0;
-    unsigned divisor = 1;
-    while (divisor < p.groups) {
-      const unsigned len_out = ((p.groups + divisor - 1) / divisor + p.sum_fanin - 1) / p.sum_fanin;
-      const dim3 grid((len_out + ACC_THREADS - 1) / ACC_THREADS, p.windows * (p.log_g + 1));
-      reduce_streams_kernel<<<grid, ACC_THREADS, 0, fs>>>(streams[si], streams[si ^ 1], p.windows, p.log_g, p.sum_fanin, divisor);
-      CHECK(cudaGetLastError());
-      launched++;
-      divisor *= p.sum_fanin;
-      si ^= 1;
-    }
+    const int si = p.log_g & 1;
     const unsigned gather_threads = p.windows * RESULT_BITS;
     batch_gather_kernel<<<(gather_threads + 127) / 128, 128, 0, fs>>>(streams[si], gb, gf, reinterpret_cast<const unsigned *>(at(grp.members_dev)),
                                                                       p.windows, p.c, p.log_m, p.log_g, io);

@@ -83,7 +83,6 @@ plan make_plan(unsigned n, unsigned window_bits, int sms) {
   p.log_m = std::min(3u, p.log_b);
   p.log_g = p.log_b - p.log_m;
   p.groups = 1u << p.log_g;
-  p.sum_fanin = 8;
   return p;
 }
 
@@ -309,28 +308,16 @@ static cudaError_t enqueue_reduction(const plan &p, const xyzz *buckets, const u
                                                                                                      p.log_m, tree[0], streams[0]);
   CHECK(cudaGetLastError());
   m.launched++;
-  int t = 0;
   for (unsigned level = 0; level < p.log_g; level++) {
-    const unsigned threads = p.windows * ((1u << p.log_g) >> (level + 1));
-    reduce_tree_kernel<<<(threads + ACC_THREADS - 1) / ACC_THREADS, ACC_THREADS, 0, stream>>>(tree[t], tree[t ^ 1], streams[0], p.windows,
-                                                                                               p.log_g, level);
+    const unsigned threads = p.windows * (level + 2) * ((1u << p.log_g) >> (level + 1));
+    const int in = level & 1;
+    reduce_level_kernel<<<(threads + ACC_THREADS - 1) / ACC_THREADS, ACC_THREADS, 0, stream>>>(tree[in], tree[in ^ 1], streams[in], streams[in ^ 1],
+                                                                                                p.windows, p.log_g, level);
     CHECK(cudaGetLastError());
     m.launched++;
-    t ^= 1;
   }
-  int s = 0;
-  unsigned divisor = 1;
-  while (divisor < p.groups) {
-    const unsigned len_out = ((p.groups + divisor - 1) / divisor + p.sum_fanin - 1) / p.sum_fanin;
-    const dim3 grid((len_out + ACC_THREADS - 1) / ACC_THREADS, p.windows * (p.log_g + 1));
-    reduce_streams_kernel<<<grid, ACC_THREADS, 0, stream>>>(streams[s], streams[s ^ 1], p.windows, p.log_g, p.sum_fanin, divisor);
-    CHECK(cudaGetLastError());
-    m.launched++;
-    divisor *= p.sum_fanin;
-    s ^= 1;
-  }
-  gather_results_kernel<<<(RESULT_BITS + 127) / 128, 128, 0, stream>>>(streams[s], buckets, flags, p.windows, p.c, p.log_m, p.log_g,
-                                                                       divisor, results);
+  gather_results_kernel<<<(RESULT_BITS + 127) / 128, 128, 0, stream>>>(streams[p.log_g & 1], buckets, flags, p.windows, p.c, p.log_m, p.log_g,
+                                                                       results);
   CHECK(cudaGetLastError());
   m.launched++;
   CHECK(m.mark(stream));
@@ -584,8 +571,7 @@ cudaError_t set_up() {
   CHECK(set_carveout(accumulate_kernel, ACC_CARVEOUT)); // 4 blocks x 18 KB of base-point slots
   CHECK(set_carveout(merge_heads_kernel, cudaSharedmemCarveoutMaxL1));
   CHECK(set_carveout(reduce_groups_kernel, cudaSharedmemCarveoutMaxL1));
-  CHECK(set_carveout(reduce_tree_kernel, cudaSharedmemCarveoutMaxL1));
-  CHECK(set_carveout(reduce_streams_kernel, cudaSharedmemCarveoutMaxL1));
+  CHECK(set_carveout(reduce_level_kernel, cudaSharedmemCarveoutMaxL1));
   return cudaSuccess;
 }
 

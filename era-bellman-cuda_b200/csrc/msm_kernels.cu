@@ -249,55 +249,43 @@ __global__ void __launch_bounds__(ACC_THREADS) reduce_groups_kernel(const xyzz *
   store_xyzz(streams + (size_t)w * stream_stride(log_g) + stream_offset(log_g, 0) + g, acc);
 }
 
-// Tree level `level`: T_{level} has G >> level entries per window (stride G).
-// Odd entries go to stream level + 1; pair sums form T_{level+1}.
-__global__ void __launch_bounds__(ACC_THREADS) reduce_tree_kernel(const xyzz *__restrict__ t_in, xyzz *__restrict__ t_out,
-                                                                  xyzz *__restrict__ streams, unsigned windows, unsigned log_g,
-                                                                  unsigned level) {
+// Level `level` of the reduction tail (log_g launches per reduction).  Per
+// window, T_level holds G >> level pair sums of the group totals run_g
+// (T_0 = run_g), and every stream s <= level holds G >> level partial sums:
+//   * the tree step writes the odd entries of T_level raw as the new stream
+//     level + 1 (the run_g with bit `level` of g set, summed in pairs so far)
+//     and the pair sums as T_level+1;
+//   * every older stream takes one pairwise step, G >> level -> G >> (level+1).
+// All streams therefore shrink together and hold one sum each after the last
+// level.  Streams and tree are ping-ponged between levels (in = level & 1).
+__global__ void __launch_bounds__(ACC_THREADS) reduce_level_kernel(const xyzz *__restrict__ t_in, xyzz *__restrict__ t_out,
+                                                                   const xyzz *__restrict__ s_in, xyzz *__restrict__ s_out, unsigned windows,
+                                                                   unsigned log_g, unsigned level) {
   const unsigned half = (1u << log_g) >> (level + 1);
+  const unsigned jobs = level + 2; // streams 0..level, then the tree
   const unsigned gid = blockIdx.x * blockDim.x + threadIdx.x;
-  if (gid >= windows * half)
+  if (gid >= windows * jobs * half)
     return;
-  const unsigned w = gid / half, i = gid % half;
+  const unsigned w = gid / (jobs * half), r = gid % (jobs * half);
+  const unsigned job = r / half, i = r % half;
   const size_t g = (size_t)1 << log_g;
-  const xyzz a = load_xyzz(t_in + w * g + 2 * i);
-  const xyzz b = load_xyzz(t_in + w * g + 2 * i + 1);
-  store_xyzz(streams + (size_t)w * stream_stride(log_g) + stream_offset(log_g, level + 1) + i, b);
-  if (level + 1 < log_g)
-    store_xyzz(t_out + w * g + i, curve::add(a, b));
-}
-
-// One plain-sum pass: every stream of length L (as of divisor_in) shrinks to
-// ceil(L / fanin); layout unchanged.
-__global__ void __launch_bounds__(ACC_THREADS) reduce_streams_kernel(const xyzz *__restrict__ in, xyzz *__restrict__ out, unsigned windows,
-                                                                     unsigned log_g, unsigned fanin, unsigned divisor_in) {
-  const unsigned streams_per_window = log_g + 1;
-  const unsigned sid = blockIdx.y;
-  const unsigned w = sid / streams_per_window, s = sid % streams_per_window;
-  if (w >= windows)
-    return;
-  const unsigned len0 = stream_length(log_g, s);
-  const unsigned len_in = (len0 + divisor_in - 1) / divisor_in;
-  const unsigned len_out = (len_in + fanin - 1) / fanin;
-  const unsigned q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= len_out)
-    return;
-  const size_t base = (size_t)w * stream_stride(log_g) + stream_offset(log_g, s);
-  xyzz acc = curve::infinity();
-  for (unsigned f = 0; f < fanin; f++) {
-    const unsigned k = q * fanin + f;
-    if (k < len_in)
-      acc = curve::add(acc, load_xyzz(in + base + k));
+  const size_t sbase = (size_t)w * stream_stride(log_g);
+  if (job <= level) {
+    const size_t o = sbase + stream_offset(log_g, job);
+    store_xyzz(s_out + o + i, curve::add(load_xyzz(s_in + o + 2 * i), load_xyzz(s_in + o + 2 * i + 1)));
+  } else {
+    const xyzz a = load_xyzz(t_in + w * g + 2 * i);
+    const xyzz b = load_xyzz(t_in + w * g + 2 * i + 1);
+    store_xyzz(s_out + sbase + stream_offset(log_g, level + 1) + i, b);
+    if (level + 1 < log_g)
+      store_xyzz(t_out + w * g + i, curve::add(a, b));
   }
-  store_xyzz(out + base + q, acc);
 }
 
 // Result bit i = c*w + o:  o == 0 -> stream 0;  o == c-1 -> slot 0 (|d| = B);
 // log_m <= o < c-1 -> stream o - log_m + 1;  otherwise infinity.
 __global__ void gather_results_kernel(const xyzz *__restrict__ streams, const xyzz *__restrict__ buckets, const uint8_t *__restrict__ flags,
-                                      unsigned windows, unsigned c, unsigned log_m, unsigned log_g, unsigned divisor,
-                                      jacobian *__restrict__ results) {
-  (void)divisor;
+                                      unsigned windows, unsigned c, unsigned log_m, unsigned log_g, jacobian *__restrict__ results) {
   const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= RESULT_BITS)
     return;

@@ -60,7 +60,6 @@ struct plan {
   unsigned log_m;       // log2 of the running-sum group
   unsigned groups;      // G = B / m groups per window
   unsigned log_g;       // gamma = log2 G
-  unsigned sum_fanin;   // fan-in of the plain-sum passes
 };
 
 // ---------------------------------------------------------------------------
@@ -120,13 +119,11 @@ __global__ void merge_chunk_buckets_kernel(xyzz *__restrict__ buckets, uint8_t *
 // ---------------------------------------------------------------------------
 __global__ void reduce_groups_kernel(const xyzz *__restrict__ buckets, const uint8_t *__restrict__ flags, unsigned windows, unsigned log_b,
                                      unsigned log_m, xyzz *__restrict__ run, xyzz *__restrict__ streams);
-__global__ void reduce_tree_kernel(const xyzz *__restrict__ t_in, xyzz *__restrict__ t_out, xyzz *__restrict__ streams, unsigned windows,
-                                   unsigned log_g, unsigned level);
-__global__ void reduce_streams_kernel(const xyzz *__restrict__ in, xyzz *__restrict__ out, unsigned windows, unsigned log_g, unsigned fanin,
-                                      unsigned divisor_in);
+// one level of the tree and of every live stream (see msm_kernels.cu)
+__global__ void reduce_level_kernel(const xyzz *__restrict__ t_in, xyzz *__restrict__ t_out, const xyzz *__restrict__ s_in, xyzz *__restrict__ s_out,
+                                    unsigned windows, unsigned log_g, unsigned level);
 __global__ void gather_results_kernel(const xyzz *__restrict__ streams, const xyzz *__restrict__ buckets, const uint8_t *__restrict__ flags,
-                                      unsigned windows, unsigned c, unsigned log_m, unsigned log_g, unsigned divisor,
-                                      jacobian *__restrict__ results);
+                                      unsigned windows, unsigned c, unsigned log_m, unsigned log_g, jacobian *__restrict__ results);
 
 // stride of the per-window plain-sum streams (stream 0: G entries, stream s: G >> s)
 __host__ __device__ __forceinline__ size_t stream_stride(unsigned log_g) { return (size_t)2 << log_g; }

@@ -16,7 +16,7 @@ def key_slot(key, B):
     return (key + 1) & (B - 1)
 
 
-def model_msm(scal, kl, c, T, chunk=4, log_m_max=4):
+def model_msm(scal, kl, c, T, chunk=4, log_m_max=3):
     n = len(scal)
     W = (254 + c - 1) // c
     log_b = c - 1
@@ -137,11 +137,17 @@ def model_msm(scal, kl, c, T, chunk=4, log_m_max=4):
             if g > 0:
                 r_ = (r_ + buckets.get((w << log_b) + g * m, 0)) % R
             run[g], accs[g] = r_, a_
+        # reduce_level_kernel: at each level every live stream takes one
+        # pairwise step and the tree's odd entries start a new stream, so all
+        # streams shrink together to one sum each
         streams, t0 = [accs], run
-        for _ in range(log_g):
+        for level in range(log_g):
+            assert all(len(st) == G >> level for st in streams)
+            streams = [[(st[2 * i] + st[2 * i + 1]) % R for i in range(len(st) // 2)] for st in streams]
             streams.append(t0[1::2])
             t0 = [(t0[2 * i] + t0[2 * i + 1]) % R for i in range(len(t0) // 2)]
-        sums = [sum(s) % R for s in streams]
+        assert all(len(st) == 1 for st in streams)
+        sums = [st[0] for st in streams]
         for o in range(c):
             val = 0
             if o == 0:
