@@ -53,6 +53,10 @@ REF_LIB = os.path.join(REPO, "oracle", "_ref", "libbellman-cuda-ref.so")
 MEASURED_PEAKS = os.path.join(REPO, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 MADD_MULOPS = 2392  # 6 mul (264) + 2 sqr (208) + one a*b - c*d (392) per XYZZ += affine
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one accumulate_kernel launch per
+# nonzero entry it processes, from the ncu --set full capture of the 2^21 uniform case
+# (2.753 GB over 33.5 M entries); a launch's traffic grows with the entries it gathers.
+ACC_DRAM_BYTES_PER_ENTRY = 82.1
 
 
 def parse():
@@ -500,7 +504,9 @@ def main():
             "peak": round(peak / 1e12, 3),
             "unit": "T mul-instr/s",
             "frac": round(achieved / peak, 4),
-            "traffic": None,
+            "traffic": round(ACC_DRAM_BYTES_PER_ENTRY * prof.nonzero_entries),
+            "traffic_source": "ncu capture at 2^21 (dram__bytes_read.sum + dram__bytes_write.sum per launch), scaled by the nonzero "
+                              "entries of this launch",
             "work": f"{prof.madds} XYZZ+affine additions x {MADD_MULOPS} 32-bit multiply instructions",
             "peak_source": "measured in this run: max of msm_b200_measure_mul_throughput kinds 4 (independent mad.lo) and 1 (paired "
                            "mad.lo.cc/madc.hi.cc chains), i.e. ~64 multiply instructions per clock per SM",
