@@ -54,9 +54,9 @@ MEASURED_PEAKS = os.path.join(REPO, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 MADD_MULOPS = 2392  # 6 mul (264) + 2 sqr (208) + one a*b - c*d (392) per XYZZ += affine
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one accumulate_kernel launch per
-# nonzero entry it processes, from the ncu --set full capture of the 2^21 uniform case
-# (2.753 GB over 33.5 M entries); a launch's traffic grows with the entries it gathers.
-ACC_DRAM_BYTES_PER_ENTRY = 82.1
+# nonzero entry it processes, from the ncu --set full capture of the 2^21 uniform case at
+# c = 17 (2.678 GB over 31.46 M entries); a launch's traffic grows with the entries it gathers.
+ACC_DRAM_BYTES_PER_ENTRY = 85.1
 
 
 def parse():
@@ -71,6 +71,9 @@ def parse():
     ap.add_argument("--no-batched", action="store_true", help="skip the 64-instance batch")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving run")
     ap.add_argument("--serving-requests", type=int, default=200, help="requests per rate (the full config: 10000)")
+    ap.add_argument("--batched-only", action="store_true",
+                    help="profiling aid: run only the batched section (--steps executions) and print its object")
+    ap.add_argument("--batched-scale", type=int, default=1, help="with --batched-only: divide every instance length by this")
     return ap.parse_args()
 
 
@@ -225,14 +228,14 @@ def generated_table(bc, seed: int, n: int, stream) -> int:
     return bd
 
 
-def batched_section(ours, bc, pool, stream, steps: int, warmup: int) -> dict:
+def batched_section(ours, bc, pool, stream, steps: int, warmup: int, scale: int = 1) -> dict:
     """The uneven 64-instance batch (lengths log-uniform in [2^10, 2^22], seed 3;
     even instances uniform, odd ones skewed; prefixes of one resident 2^22-point
     table): one execution of the batched graph against 64 sequential plain calls
     (for the reference: 64 calls padded with zero scalars to powers of two)."""
     import synth
-    lengths = [int(x) for x in synth.batch_lengths(3, 64)]
-    n_table = 1 << 22
+    lengths = [max(1, int(x) // scale) for x in synth.batch_lengths(3, 64)]
+    n_table = (1 << 22) // scale
     table_dev = generated_table(ours, 3, n_table, stream)
     work = [s for _, s in synth.batch_workload(3, lengths)]
     points = sum(lengths)
@@ -394,6 +397,12 @@ def main():
         return
     ours = bcm.BellmanCuda()  # generates the inputs in both arms
     ours.set_device(dist.local)
+    if args.batched_only:
+        ours.msm_set_up()
+        pool, stream = ours.mem_pool_create(dist.local), ours.stream_create(True)
+        print(json.dumps(batched_section(ours, ours, pool, stream, args.steps, max(args.warmup, 3), args.batched_scale)))
+        dist.close()
+        return
     bc = ours if args.impl == "b200" else bcm.BellmanCuda(REF_LIB)
     bc.set_device(dist.local)
     bc.ff_set_up(25, 14)
