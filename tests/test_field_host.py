@@ -157,3 +157,38 @@ def test_curve_identities(field_check, oracle):
         jac = np.zeros(24, np.uint32)
         f.fc_to_jacobian(ptr(q), ptr(jac))
         assert oracle.normalize(jac) == (False, *table[2 * i + 1])
+
+
+def full_words(rng, count):
+    """Uniform 256-bit words and the carry corner cases of the 128-bit halves."""
+    vals = [int.from_bytes(rng.bytes(32), "little") for _ in range(count)]
+    corners = [0, 1, (1 << 256) - 1, (1 << 128) - 1, 1 << 128, ((1 << 128) - 1) << 128, (1 << 255) | 1, 2 * P - 1, P]
+    return vals + corners
+
+
+@pytest.mark.parametrize("kind", [0, 1])
+def test_wide_products_exact(field_check, kind):
+    """Schoolbook and Karatsuba 512-bit products against Python integers, on
+    arbitrary 256-bit operands (both halves' differences of either sign)."""
+    rng = np.random.Generator(np.random.PCG64(11 + kind))
+    xs = full_words(rng, 3000)
+    ys = list(reversed(full_words(rng, 3000)))
+    pairs_ = [(x, y) for x in xs[-9:] for y in ys[:9]] + list(zip(xs, ys))
+    a, b = arr([p[0] for p in pairs_]), arr([p[1] for p in pairs_])
+    out = np.zeros(16 * len(pairs_), np.uint32)
+    field_check.fc_fq_wide(kind, ptr(a), ptr(b), ptr(out), len(pairs_))
+    for (x, y), got in zip(pairs_, ints(out, 16)):
+        assert got == x * y
+
+
+def test_karatsuba_montgomery_matches_cios(field_check, pairs):
+    """Both Montgomery products give the same lazy residue class and range."""
+    xs, ys = pairs
+    a, b = arr(xs), arr(ys)
+    out_c = np.zeros_like(a)
+    out_k = np.zeros_like(a)
+    field_check.fc_fq_wide(3, ptr(a), ptr(b), ptr(out_c), len(xs))
+    field_check.fc_fq_wide(4, ptr(a), ptr(b), ptr(out_k), len(xs))
+    for x, y, c_, k_ in zip(xs, ys, ints(out_c), ints(out_k)):
+        assert c_ < 2 * P and k_ < 2 * P
+        assert c_ % P == k_ % P == x * y * RINV % P
