@@ -193,6 +193,9 @@ class BellmanCuda:
                 "msm_b200_base_table_create": [ctypes.POINTER(vp), vp, u, ctypes.POINTER(u), u, Handle],
                 "msm_b200_base_table_bytes": [vp, ctypes.POINTER(sz)],
                 "msm_b200_base_table_destroy": [vp],
+                "msm_b200_base_table_serialized_bytes": [vp, ctypes.POINTER(sz)],
+                "msm_b200_base_table_export": [vp, vp, sz],
+                "msm_b200_base_table_import": [ctypes.POINTER(vp), vp, sz, Handle],
                 "msm_b200_batch_window_bits": [u, ctypes.POINTER(u)],
                 "msm_b200_batch_create": [ctypes.POINTER(vp), vp, ctypes.POINTER(u), u, ctypes.POINTER(u)],
                 "msm_b200_batch_execute_async": [vp, ctypes.POINTER(vp), ctypes.POINTER(vp), Handle],
@@ -409,6 +412,21 @@ class BellmanCuda:
 
     def base_table_destroy(self, table: int) -> None:
         self.check(self.lib.msm_b200_base_table_destroy(table), "msm_b200_base_table_destroy")
+
+    def base_table_export(self, table: int) -> np.ndarray:
+        """The table's save format as a uint8 array."""
+        n = ctypes.c_size_t()
+        self.check(self.lib.msm_b200_base_table_serialized_bytes(table, ctypes.byref(n)), "msm_b200_base_table_serialized_bytes")
+        img = np.zeros(n.value, np.uint8)
+        self.check(self.lib.msm_b200_base_table_export(table, img.ctypes.data, n.value), "msm_b200_base_table_export")
+        return img
+
+    def base_table_import_raw(self, image: np.ndarray, stream: Handle):
+        """(bc_error, handle) of msm_b200_base_table_import."""
+        h = ctypes.c_void_p()
+        image = np.ascontiguousarray(image, dtype=np.uint8)
+        rc = self.lib.msm_b200_base_table_import(ctypes.byref(h), image.ctypes.data, image.nbytes, stream)
+        return rc, h.value
 
     def batch_window_bits(self, count: int) -> int:
         c = ctypes.c_uint()

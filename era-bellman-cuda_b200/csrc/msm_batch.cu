@@ -30,7 +30,6 @@
 #include <cstring>
 #include <map>
 #include <memory>
-#include <mutex>
 #include <new>
 #include <vector>
 
@@ -149,7 +148,7 @@ __global__ void __launch_bounds__(256) batch_sort_scan_kernel(uint32_t *counts, 
 }
 
 template <bool STABLE>
-__global__ void __launch_bounds__(SORT_THREADS, STABLE ? 2 : 3) batch_sort_scatter_kernel(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
+__global__ void __launch_bounds__(SORT_THREADS, 3) batch_sort_scatter_kernel(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
                                                                           uint32_t *__restrict__ keys_out, uint32_t *__restrict__ vals_out,
                                                                           const batch_instance *__restrict__ inst,
                                                                           const unsigned *__restrict__ tile_seg, unsigned shift,
@@ -317,7 +316,95 @@ cudaError_t base_table_create(base_table_impl **out, const void *bases, unsigned
   return cudaSuccess;
 }
 
+// Serialised table: a little-endian header (magic, version, point count,
+// number of widths, then per width: c, prefix, windows) followed, width by
+// width in increasing c, by the W(c) x prefix affine points (Montgomery form,
+// 64 B each) of M_c.  Importing it skips the precomputation.
+constexpr uint32_t TABLE_MAGIC0 = 0x34354e42; // "BN54"
+constexpr uint32_t TABLE_MAGIC1 = 0x4c424154; // "TABL"
+constexpr uint32_t TABLE_VERSION = 1;
 
+static size_t table_header_bytes(unsigned widths) { return (size_t)(5 + 3 * widths) * sizeof(uint32_t); }
+
+size_t base_table_serialized_bytes(const base_table_impl &t) {
+  unsigned widths = 0;
+  size_t bytes = 0;
+  for (unsigned c = 2; c <= MAX_TABLE_BITS; c++)
+    if (t.mult[c]) {
+      widths++;
+      bytes += (size_t)windows_for(c) * t.prefix[c] * sizeof(affine);
+    }
+  return table_header_bytes(widths) + bytes;
+}
+
+cudaError_t base_table_export(const base_table_impl &t, void *out, size_t bytes) {
+  if (!out || bytes < base_table_serialized_bytes(t))
+    return cudaErrorInvalidValue;
+  std::vector<uint32_t> header = {TABLE_MAGIC0, TABLE_MAGIC1, TABLE_VERSION, t.count};
+  std::vector<unsigned> widths;
+  for (unsigned c = 2; c <= MAX_TABLE_BITS; c++)
+    if (t.mult[c])
+      widths.push_back(c);
+  header.push_back((uint32_t)widths.size());
+  for (unsigned c : widths) {
+    header.push_back(c);
+    header.push_back(t.prefix[c]);
+    header.push_back(windows_for(c));
+  }
+  uint8_t *dst = static_cast<uint8_t *>(out);
+  // the header: magic (2 words), version, count, widths, then the per-width triples
+  std::memcpy(dst, header.data(), header.size() * sizeof(uint32_t));
+  dst += header.size() * sizeof(uint32_t);
+  for (unsigned c : widths) {
+    const size_t n = (size_t)windows_for(c) * t.prefix[c] * sizeof(affine);
+    CHECK(cudaMemcpy(dst, t.mult[c], n, cudaMemcpyDeviceToHost));
+    dst += n;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t base_table_import(base_table_impl **out, const void *image, size_t bytes, cudaStream_t stream) {
+  if (!out || !image || bytes < 5 * sizeof(uint32_t))
+    return cudaErrorInvalidValue;
+  const uint32_t *h = static_cast<const uint32_t *>(image);
+  if (h[0] != TABLE_MAGIC0 || h[1] != TABLE_MAGIC1 || h[2] != TABLE_VERSION || h[3] == 0)
+    return cudaErrorInvalidValue;
+  const unsigned count = h[3], widths = h[4];
+  if (widths == 0 || widths > MAX_TABLE_BITS || bytes < table_header_bytes(widths))
+    return cudaErrorInvalidValue;
+  const uint32_t *w = h + 5; // per-width triples
+  size_t need = table_header_bytes(widths);
+  unsigned last_c = 1;
+  for (unsigned k = 0; k < widths; k++) {
+    const unsigned c = w[3 * k], prefix = w[3 * k + 1], windows = w[3 * k + 2];
+    if (c <= last_c || c > MAX_TABLE_BITS || prefix == 0 || prefix > count || windows != windows_for(c))
+      return cudaErrorInvalidValue;
+    last_c = c;
+    need += (size_t)windows * prefix * sizeof(affine);
+  }
+  if (bytes < need)
+    return cudaErrorInvalidValue;
+  std::unique_ptr<base_table_impl> t(new (std::nothrow) base_table_impl);
+  if (!t)
+    return cudaErrorMemoryAllocation;
+  CHECK(cudaGetDevice(&t->device));
+  t->count = count;
+  const uint8_t *src = reinterpret_cast<const uint8_t *>(w + 3 * widths);
+  for (unsigned k = 0; k < widths; k++) {
+    const unsigned c = w[3 * k], prefix = w[3 * k + 1];
+    const size_t n = (size_t)windows_for(c) * prefix * sizeof(affine);
+    affine *m = nullptr;
+    CHECK(cudaMalloc(&m, n));
+    t->mult[c] = m;
+    t->prefix[c] = prefix;
+    t->bytes += n;
+    CHECK(cudaMemcpyAsync(m, src, n, cudaMemcpyHostToDevice, stream));
+    src += n;
+  }
+  CHECK(cudaStreamSynchronize(stream));
+  *out = t.release();
+  return cudaSuccess;
+}
 
 cudaError_t make_batch_plan(batch_plan &b, const base_table_impl *table, const unsigned *counts, unsigned instances, const unsigned *window_bits,
                             int sms) {
@@ -658,6 +745,28 @@ bc_error msm_b200_base_table_bytes(msm_b200_base_table table, size_t *bytes) {
     return bc_error_invalid_value;
   *bytes = reinterpret_cast<msm_b200::base_table_impl *>(table)->bytes;
   return bc_success;
+}
+
+bc_error msm_b200_base_table_serialized_bytes(msm_b200_base_table table, size_t *bytes) {
+  if (!table || !bytes)
+    return bc_error_invalid_value;
+  *bytes = msm_b200::base_table_serialized_bytes(*reinterpret_cast<msm_b200::base_table_impl *>(table));
+  return bc_success;
+}
+
+bc_error msm_b200_base_table_export(msm_b200_base_table table, void *image, size_t bytes) {
+  if (!table)
+    return bc_error_invalid_value;
+  return static_cast<bc_error>(msm_b200::base_table_export(*reinterpret_cast<msm_b200::base_table_impl *>(table), image, bytes));
+}
+
+bc_error msm_b200_base_table_import(msm_b200_base_table *table, const void *image, size_t bytes, bc_stream stream) {
+  if (!table)
+    return bc_error_invalid_value;
+  msm_b200::base_table_impl *t = nullptr;
+  const cudaError_t e = msm_b200::base_table_import(&t, image, bytes, static_cast<cudaStream_t>(stream.handle));
+  *table = reinterpret_cast<msm_b200_base_table>(t);
+  return static_cast<bc_error>(e);
 }
 
 bc_error msm_b200_base_table_destroy(msm_b200_base_table table) {

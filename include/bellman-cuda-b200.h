@@ -97,6 +97,17 @@ bc_error msm_b200_base_table_create(msm_b200_base_table *table, const void *base
 /* Device bytes the table holds. */
 bc_error msm_b200_base_table_bytes(msm_b200_base_table table, size_t *bytes);
 bc_error msm_b200_base_table_destroy(msm_b200_base_table table);
+/* Save / load format of a table: a little-endian header (the words
+ * 0x34354e42 0x4c424154, version 1, point count, number of widths, then per
+ * width c, prefix, windows) followed by each width's windows x prefix affine
+ * points (Montgomery form, 64 B each), widths in increasing order.  Export
+ * writes it into host memory of msm_b200_base_table_serialized_bytes bytes
+ * (synchronous); import rebuilds the table on the current device without
+ * recomputing the multiples and rejects a malformed or truncated image with
+ * bc_error_invalid_value. */
+bc_error msm_b200_base_table_serialized_bytes(msm_b200_base_table table, size_t *bytes);
+bc_error msm_b200_base_table_export(msm_b200_base_table table, void *image, size_t bytes);
+bc_error msm_b200_base_table_import(msm_b200_base_table *table, const void *image, size_t bytes, bc_stream stream);
 
 /* The window width the batched path uses for an instance of `count` points:
  * the checked-in table written by the autotuner (era-bellman-cuda_b200/autotune.py). */

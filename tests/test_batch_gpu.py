@@ -2,8 +2,8 @@
 msm_b200_batch_*), through the C ABI: every instance's Horner-reduced,
 normalised point equals the oracle's checksum MSM and the plain entry point's
 result on the same inputs (bit-exact), for tuned and forced window widths,
-re-executions with new scalar/result buffers, and the full 64-instance batch
-of lengths log-uniform in [2^10, 2^22] (seed 3)."""
+re-executions with new scalar/result buffers, a table saved and loaded back,
+and the full 64-instance batch of lengths log-uniform in [2^10, 2^22] (seed 3)."""
 import pytest
 
 import synth
@@ -130,6 +130,27 @@ def test_batch_invalid_arguments(lib, table16):
     assert bc.batch_create_raw(table, [(1 << 16) + 1])[0] == 1  # longer than the table
     assert bc.batch_create_raw(table, [10], window_bits=[23])[0] == 1  # width not in the table
     assert bc.batch_create_raw(table, [10] * 257)[0] == 1
+
+
+def test_table_export_import(lib, oracle, table16):
+    """A table saved and loaded again (no recomputation) gives the same results;
+    truncated or corrupted images are rejected."""
+    k, _, table = table16
+    bc = lib.bc
+    img = bc.base_table_export(table)
+    rc, copy = bc.base_table_import_raw(img, lib.stream)
+    assert rc == 0
+    assert bc.base_table_bytes(copy) == bc.base_table_bytes(table)
+    assert (bc.base_table_export(copy) == img).all()
+    lengths = [65536, 999, 4]
+    work = [synth.uniform_scalars(800 + j, n) for j, n in enumerate(lengths)]
+    for a, b, n, s in zip(lib.run_batch(table, work), lib.run_batch(copy, work), lengths, work):
+        assert oracle.horner(a) == oracle.horner(b) == oracle.msm_checksum(k[:n], s)
+    bc.base_table_destroy(copy)
+    assert bc.base_table_import_raw(img[: len(img) - 64], lib.stream)[0] == 1
+    bad = img.copy()
+    bad[0] ^= 1
+    assert bc.base_table_import_raw(bad, lib.stream)[0] == 1
 
 
 def test_batch_config3_full(lib, oracle):

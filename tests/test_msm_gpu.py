@@ -260,6 +260,40 @@ def test_chunked_events_and_callbacks(gpu, oracle):
     bc.free_host(hs_ptr)
 
 
+def test_concurrent_streams_and_threads(gpu, oracle):
+    """msm_execute_async is re-entrant: MSMs on different streams, enqueued from
+    different host threads, overlap on the device and all come out right
+    (the reference's tests/bc_test.cu:126-170 does the same with its MSM)."""
+    import threading
+    bc = gpu.bc
+    jobs = []
+    for j, log_n in enumerate((12, 16, 18, 20)):
+        bases, scalars, k = H.table_workload(1 << log_n, 40 + j)
+        jobs.append((log_n, gpu.upload(bases), gpu.upload(scalars), bc.malloc(254 * 96), k, scalars, bc.stream_create(True)))
+    errors = []
+
+    def run(job):
+        log_n, bd, sd, rd, _, _, st = job
+        try:
+            for _ in range(3):
+                bc.msm(gpu.pool, st, bd, sd, rd, log_n)
+            bc.stream_synchronize(st)
+        except Exception as e:  # reported below, on the main thread
+            errors.append(e)
+
+    threads = [threading.Thread(target=run, args=(job,)) for job in jobs]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not errors, errors
+    for log_n, bd, sd, rd, k, scalars, st in jobs:
+        assert oracle.horner(bc.from_device(rd, (254, 24))) == oracle.msm_checksum(k, scalars), f"2^{log_n}"
+        for p in (bd, sd, rd):
+            bc.free(p)
+        bc.stream_destroy(st)
+
+
 def test_invalid_arguments(gpu):
     bc = gpu.bc
     res = np.zeros((254, 24), np.uint32)
