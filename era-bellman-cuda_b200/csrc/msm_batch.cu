@@ -190,7 +190,7 @@ struct table_segments {
 
 __global__ void __launch_bounds__(ACC_THREADS, ACC_MIN_BLOCKS) batch_accumulate_kernel(
     const uint32_t *__restrict__ keys, const uint32_t *__restrict__ vals, const batch_instance *__restrict__ inst, unsigned instances,
-    const uint32_t *__restrict__ zeros, unsigned total_threads, xyzz *__restrict__ buckets, uint8_t *__restrict__ flags,
+    const uint32_t *__restrict__ zeros, unsigned ranges, unsigned *__restrict__ work, xyzz *__restrict__ buckets, uint8_t *__restrict__ flags,
     uint32_t *__restrict__ head_bucket, xyzz *__restrict__ head_point) {
   __shared__ unsigned long long s_first[MAX_BATCH], s_end[MAX_BATCH], s_prefix[MAX_BATCH + 1];
   __shared__ uint32_t s_bucket[MAX_BATCH], s_mask[MAX_BATCH];
@@ -215,7 +215,7 @@ __global__ void __launch_bounds__(ACC_THREADS, ACC_MIN_BLOCKS) batch_accumulate_
   }
   __syncthreads();
   const table_segments seg{s_first, s_end, s_prefix, s_bucket, s_mask, s_table, instances};
-  accumulate_ranges(seg, keys, vals, total_threads, buckets, flags, head_bucket, head_point, s_base);
+  accumulate_ranges(seg, keys, vals, ranges, work, buckets, flags, head_bucket, head_point, s_base);
 }
 
 // Results of the instances of one reduction group (all of window width c):
@@ -461,6 +461,7 @@ cudaError_t make_batch_plan(batch_plan &b, const base_table_impl *table, const u
   }
   const unsigned long long full = (unsigned long long)sms * ACC_MIN_BLOCKS * ACC_THREADS;
   b.acc_threads = (unsigned)std::max(1ull, std::min(full, (b.total_entries + 7) / 8));
+  b.acc_ranges = accumulation_ranges(b.acc_threads, b.total_entries, BATCH_ACC_RANGES_PER_THREAD);
   // scratch layout
   size_t off = 0;
   auto take = [&](size_t bytes) {
@@ -478,9 +479,10 @@ cudaError_t make_batch_plan(batch_plan &b, const base_table_impl *table, const u
   b.buckets = take((size_t)b.slots * sizeof(xyzz));
   b.flags = take(b.slots);
   for (int i = 0; i < 2; i++) {
-    b.hb[i] = take((size_t)b.acc_threads * 4);
-    b.hp[i] = take((size_t)b.acc_threads * sizeof(xyzz));
+    b.hb[i] = take((size_t)b.acc_ranges * 4);
+    b.hp[i] = take((size_t)b.acc_ranges * sizeof(xyzz));
   }
+  b.work = take(sizeof(unsigned));
   for (batch_group &g : b.groups)
     for (int i = 0; i < 2; i++) {
       g.tree[i] = take(((size_t)g.p.windows << g.p.log_g) * sizeof(xyzz));
@@ -558,11 +560,13 @@ cudaError_t enqueue_batch(const batch_plan &b, uint8_t *scratch, cudaStream_t s,
     launched += 3;
     cur ^= 1;
   }
+  unsigned *work = reinterpret_cast<unsigned *>(at(b.work));
+  CHECK(cudaMemsetAsync(work, 0, sizeof(unsigned), s));
   batch_accumulate_kernel<<<(b.acc_threads + ACC_THREADS - 1) / ACC_THREADS, ACC_THREADS, 0, s>>>(
-      keys[cur], vals[cur], inst, b.instances, zeros, b.acc_threads, buckets, flags, hb[0], hp[0]);
+      keys[cur], vals[cur], inst, b.instances, zeros, b.acc_ranges, work, buckets, flags, hb[0], hp[0]);
   CHECK(cudaGetLastError());
   launched++;
-  unsigned heads = b.acc_threads;
+  unsigned heads = b.acc_ranges;
   int h = 0;
   while (heads > 1) {
     const unsigned out = (heads + 3) / 4;

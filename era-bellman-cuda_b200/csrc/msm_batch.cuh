@@ -57,11 +57,11 @@ struct batch_group {
 struct batch_plan {
   unsigned instances = 0;
   unsigned long long total_entries = 0;
-  unsigned total_points = 0, total_tiles = 0, slots = 0, sort_passes = 0, acc_threads = 0;
+  unsigned total_points = 0, total_tiles = 0, slots = 0, sort_passes = 0, acc_threads = 0, acc_ranges = 0;
   std::vector<batch_instance> inst;
   std::vector<unsigned> point_offset;
   std::vector<batch_group> groups;
-  size_t keys[2], vals[2], counts, totals, zeros, buckets, flags, hb[2], hp[2], inst_dev, point_offset_dev, tile_seg_dev, io;
+  size_t keys[2], vals[2], counts, totals, zeros, buckets, flags, hb[2], hp[2], work, inst_dev, point_offset_dev, tile_seg_dev, io;
   size_t bytes = 0;       // scratch bytes
   size_t descriptors = 0; // offset of the constant descriptors (inst_dev .. end of members)
 };

@@ -343,13 +343,16 @@ template <int PENDING> __device__ __forceinline__ void cp_async_wait() { asm vol
 
 // Bucket accumulation over a list of segments of sorted (key, value) entries.
 // The nonzero entries of all segments form one virtual list of M entries,
-// split into equal contiguous ranges, one per thread (total_threads).  Each
-// thread walks its range, gathers the signed affine base of every entry
-// (double-buffered through shared memory by cp.async), starts a new XYZZ
-// accumulator when the bucket changes and otherwise does one mixed addition.
-// A bucket that starts inside the range is written directly (and flagged); a
-// bucket continued from the previous range leaves a "head" partial sum for
-// merge_heads_kernel.  SEG describes the segments (all methods device-side):
+// split into `ranges` equal contiguous ranges.  Warps take 32 consecutive
+// ranges at a time from a work counter (one range per lane, lengths equal to
+// within one entry, so the lanes stay in step), which keeps every SM busy
+// until the last ranges are handed out.  A lane walks its range, gathers the
+// signed affine base of every entry (double-buffered through shared memory by
+// cp.async), starts a new XYZZ accumulator when the bucket changes and
+// otherwise does one mixed addition.  A bucket that starts inside the range is
+// written directly (and flagged); a bucket continued from the previous range
+// leaves a "head" partial sum for merge_heads_kernel.  SEG describes the
+// segments (all methods device-side):
 //   count()          segments
 //   prefix(s)        nonzero entries before segment s (s <= count())
 //   first(s), end(s) physical index of the first nonzero entry / one past the last
@@ -357,20 +360,11 @@ template <int PENDING> __device__ __forceinline__ void cp_async_wait() { asm vol
 //   bucket(s, key)   global bucket slot of a key of segment s
 //   base(s, val)     affine base of a value of segment s (sign bit ignored)
 template <class SEG>
-__device__ __forceinline__ void accumulate_ranges(const SEG &seg, const uint32_t *__restrict__ keys, const uint32_t *__restrict__ vals,
-                                                  unsigned total_threads, xyzz *__restrict__ buckets, uint8_t *__restrict__ flags,
-                                                  uint32_t *__restrict__ head_bucket, xyzz *__restrict__ head_point,
-                                                  uint4 (*s_base)[4][ACC_THREADS]) {
-  const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= total_threads)
-    return;
-  // Only the first min(total, total_threads) ranges are used, so every active
-  // range holds at least one entry and the heads of one bucket stay
-  // contiguous (an empty range between them would let two merge threads
-  // update the same bucket).
+__device__ __forceinline__ void accumulate_range(const SEG &seg, const uint32_t *__restrict__ keys, const uint32_t *__restrict__ vals, unsigned t,
+                                                 unsigned long long total, unsigned long long active, xyzz *__restrict__ buckets,
+                                                 uint8_t *__restrict__ flags, uint32_t *__restrict__ head_bucket, xyzz *__restrict__ head_point,
+                                                 uint4 (*s_base)[4][ACC_THREADS]) {
   const unsigned segments = seg.count();
-  const unsigned long long total = seg.prefix(segments);
-  const unsigned long long active = total < total_threads ? total : total_threads;
   head_bucket[t] = INVALID_BUCKET;
   if (t >= active)
     return;
@@ -495,6 +489,31 @@ __device__ __forceinline__ void accumulate_ranges(const SEG &seg, const uint32_t
   } else {
     store_xyzz(buckets + bucket, acc);
     flags[bucket] = 1;
+  }
+}
+
+// The work loop over all ranges (see accumulate_range).  Only the first
+// min(M, ranges) ranges hold entries, so every active range holds at least one
+// entry and the heads of one bucket stay contiguous (an empty range between
+// them would let two merge threads update the same bucket); every range still
+// writes its head slot.  *work must be 0 at launch; blocks are whole warps.
+template <class SEG>
+__device__ __forceinline__ void accumulate_ranges(const SEG &seg, const uint32_t *__restrict__ keys, const uint32_t *__restrict__ vals,
+                                                  unsigned ranges, unsigned *__restrict__ work, xyzz *__restrict__ buckets,
+                                                  uint8_t *__restrict__ flags, uint32_t *__restrict__ head_bucket, xyzz *__restrict__ head_point,
+                                                  uint4 (*s_base)[4][ACC_THREADS]) {
+  const unsigned long long total = seg.prefix(seg.count());
+  const unsigned long long active = total < ranges ? total : ranges;
+  const unsigned lane = threadIdx.x & 31;
+  for (;;) {
+    unsigned first = 0;
+    if (lane == 0)
+      first = atomicAdd(work, 32u);
+    first = __shfl_sync(0xffffffffu, first, 0);
+    if (first >= ranges)
+      return;
+    if (first + lane < ranges)
+      accumulate_range(seg, keys, vals, first + lane, total, active, buckets, flags, head_bucket, head_point, s_base);
   }
 }
 

@@ -64,6 +64,14 @@ static device_info get_device_info(int device) {
   return cache[device];
 }
 
+// Accumulation ranges: up to per_thread per thread, as long as a range keeps
+// at least ACC_MIN_RANGE entries (more ranges even out the end of the launch;
+// each range may leave one head to merge).
+unsigned accumulation_ranges(unsigned threads, unsigned long long entries, unsigned per_thread) {
+  const unsigned long long wanted = std::min((unsigned long long)threads * per_thread, entries / ACC_MIN_RANGE);
+  return (unsigned)std::max((unsigned long long)threads, wanted);
+}
+
 plan make_plan(unsigned n, unsigned window_bits, int sms) {
   plan p{};
   p.n = n;
@@ -78,6 +86,7 @@ plan make_plan(unsigned n, unsigned window_bits, int sms) {
   const unsigned long long entries = (unsigned long long)p.windows * n;
   const unsigned long long full = (unsigned long long)sms * 4 * ACC_THREADS;
   p.acc_threads = (unsigned)std::max(1ull, std::min(full, (entries + 7) / 8));
+  p.acc_ranges = accumulation_ranges(p.acc_threads, entries, ACC_RANGES_PER_THREAD);
   p.merge_chunk = 4;
   // groups of m = 8 slots: enough reduction threads to fill the GPU at c = 16
   p.log_m = std::min(3u, p.log_b);
@@ -93,8 +102,14 @@ plan make_plan(unsigned n, unsigned window_bits, int sms) {
 // about five times as long per point as the host-to-device copy), so only the
 // first, small chunk's copy is exposed.  Reference counterpart: the chunked
 // copy/compute overlap of schedule_execution (src/msm.cu:160-334).
-constexpr unsigned MAX_CHUNKS = 4;
-constexpr unsigned CHUNK_GROWTH = 4;
+#ifndef MSM_MAX_CHUNKS
+#define MSM_MAX_CHUNKS 4
+#endif
+#ifndef MSM_CHUNK_GROWTH
+#define MSM_CHUNK_GROWTH 4
+#endif
+constexpr unsigned MAX_CHUNKS = MSM_MAX_CHUNKS;
+constexpr unsigned CHUNK_GROWTH = MSM_CHUNK_GROWTH;
 constexpr unsigned MIN_FIRST_CHUNK = 1u << 16;
 
 struct chunking {
@@ -136,7 +151,7 @@ static chunking make_chunks(unsigned n, bool copy_inputs) {
 // host-resident inputs are sized for all `copy_n` points; a chunked MSM holds a
 // second bucket set for the chunks after the first.
 struct layout {
-  size_t keys[2], vals[2], counts, totals, zeros, buckets, flags, chunk_buckets, chunk_flags, hb[2], hp[2], tree[2], streams[2], results,
+  size_t keys[2], vals[2], counts, totals, zeros, buckets, flags, chunk_buckets, chunk_flags, hb[2], hp[2], work, tree[2], streams[2], results,
       scalars, bases, total;
 };
 
@@ -168,9 +183,10 @@ static layout make_layout(const plan &p, bool copy_scalars, bool copy_bases, boo
     l.chunk_flags = take(slots);
   }
   for (int i = 0; i < 2; i++) {
-    l.hb[i] = take((size_t)p.acc_threads * 4);
-    l.hp[i] = take((size_t)p.acc_threads * sizeof(xyzz));
+    l.hb[i] = take((size_t)p.acc_ranges * 4);
+    l.hp[i] = take((size_t)p.acc_ranges * sizeof(xyzz));
   }
+  l.work = take(sizeof(unsigned));
   for (int i = 0; i < 2; i++) {
     l.tree[i] = take(((size_t)p.windows << p.log_g) * sizeof(xyzz));
     l.streams[i] = take((size_t)p.windows * stream_stride(p.log_g) * sizeof(xyzz));
@@ -276,14 +292,16 @@ static cudaError_t enqueue_accumulation(const plan &p, const fe *scalars, const 
   CHECK(m.mark(stream));
 
   // 4. accumulation
+  unsigned *work = reinterpret_cast<unsigned *>(scratch + l.work);
+  CHECK(cudaMemsetAsync(work, 0, sizeof(unsigned), stream));
   accumulate_kernel<<<(p.acc_threads + ACC_THREADS - 1) / ACC_THREADS, ACC_THREADS, 0, stream>>>(
-      keys[cur], vals[cur], bases, n, p.windows, p.log_b, zeros, p.acc_threads, buckets, flags, hb[0], hp[0]);
+      keys[cur], vals[cur], bases, n, p.windows, p.log_b, zeros, p.acc_ranges, work, buckets, flags, hb[0], hp[0]);
   CHECK(cudaGetLastError());
   m.launched++;
   CHECK(m.mark(stream));
 
   // 5. heads
-  unsigned heads = p.acc_threads;
+  unsigned heads = p.acc_ranges;
   int h = 0;
   while (heads > 1) {
     const unsigned out = (heads + p.merge_chunk - 1) / p.merge_chunk;
@@ -354,7 +372,7 @@ static cudaError_t collect_profile(const plan &p, const layout &l, const uint8_t
   CHECK(cudaMemcpy(zeros.data(), scratch + l.zeros, zeros.size() * 4, cudaMemcpyDeviceToHost));
   std::vector<uint8_t> flags((size_t)p.windows << p.log_b);
   CHECK(cudaMemcpy(flags.data(), scratch + l.flags, flags.size(), cudaMemcpyDeviceToHost));
-  std::vector<uint32_t> heads(p.acc_threads);
+  std::vector<uint32_t> heads(p.acc_ranges);
   CHECK(cudaMemcpy(heads.data(), scratch + l.hb[0], heads.size() * 4, cudaMemcpyDeviceToHost));
   unsigned long long nonzero = 0, nonempty = 0, continued = 0;
   for (uint32_t z : zeros)
@@ -368,7 +386,7 @@ static cudaError_t collect_profile(const plan &p, const layout &l, const uint8_t
   out->heads = continued;
   out->window_bits = p.c;
   out->windows = p.windows;
-  out->acc_threads = p.acc_threads;
+  out->acc_threads = p.acc_ranges;
   out->launches = launches;
   return cudaSuccess;
 }

@@ -34,7 +34,22 @@ constexpr unsigned MAX_FUSED_HISTOGRAM_WINDOWS = 48;
 // stages timed by msm_b200_execute_profiled
 constexpr unsigned PROFILE_STAGES = 6;
 
+// Accumulation ranges per thread, handed out to warps dynamically.  Measured
+// on a B200 at 2^22: 2 per thread cut the plain accumulation from 9.85 to
+// 9.32 ms (the last ranges no longer leave SMs idle), 3 gave 9.50 (more heads
+// to merge); the batched chain measured best at 1.
+#ifndef ACC_RANGES_PER_THREAD
+#define ACC_RANGES_PER_THREAD 2
+#endif
+#ifndef BATCH_ACC_RANGES_PER_THREAD
+#define BATCH_ACC_RANGES_PER_THREAD 1
+#endif
+#ifndef ACC_MIN_RANGE
+#define ACC_MIN_RANGE 256 // entries a range keeps at least when ranges are multiplied
+#endif
+
 unsigned default_window_bits(unsigned long long n);
+unsigned accumulation_ranges(unsigned threads, unsigned long long entries, unsigned per_thread);
 plan make_plan(unsigned n, unsigned window_bits, int sms);
 size_t scratch_bytes(unsigned n, unsigned window_bits, bool copy_scalars, bool copy_bases, bool copy_results);
 cudaError_t execute(const execution &e);

@@ -138,7 +138,7 @@ struct window_segments {
 
 __global__ void __launch_bounds__(ACC_THREADS, ACC_MIN_BLOCKS) accumulate_kernel(const uint32_t *__restrict__ keys, const uint32_t *__restrict__ vals,
                                                                  const affine *__restrict__ bases, unsigned n, unsigned windows, unsigned log_b,
-                                                                 const uint32_t *__restrict__ zeros, unsigned total_threads,
+                                                                 const uint32_t *__restrict__ zeros, unsigned ranges, unsigned *__restrict__ work,
                                                                  xyzz *__restrict__ buckets, uint8_t *__restrict__ flags,
                                                                  uint32_t *__restrict__ head_bucket, xyzz *__restrict__ head_point) {
   __shared__ uint32_t s_zeros[MAX_WINDOWS];
@@ -157,7 +157,7 @@ __global__ void __launch_bounds__(ACC_THREADS, ACC_MIN_BLOCKS) accumulate_kernel
   }
   __syncthreads();
   const window_segments seg{bases, s_zeros, s_prefix, n, windows, log_b};
-  accumulate_ranges(seg, keys, vals, total_threads, buckets, flags, head_bucket, head_point, s_base);
+  accumulate_ranges(seg, keys, vals, ranges, work, buckets, flags, head_bucket, head_point, s_base);
 }
 
 // ---------------------------------------------------------------------------

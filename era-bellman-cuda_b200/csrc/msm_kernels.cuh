@@ -9,7 +9,7 @@
 //                  the first pass drops zero digits (counted per window), so
 //                  window w keeps its nonzero entries at the end of its segment
 //   4. accumulate  the nonzero entries of all windows are split into equal
-//                  contiguous ranges, one per thread; each thread adds its
+//                  contiguous ranges, handed out to warps; each thread adds its
 //                  range bucket by bucket (XYZZ += affine); buckets that start
 //                  inside a range are written directly, a bucket continued
 //                  from the previous range leaves a "head" partial sum
@@ -55,7 +55,8 @@ struct plan {
   unsigned key_bits;    // bits of a sort key (|d| - 1 for |d| in [1, 2^log_b])
   unsigned sort_passes; // radix passes
   unsigned tiles;       // sort tiles per window
-  unsigned acc_threads; // accumulation threads (ranges)
+  unsigned acc_threads; // accumulation threads (4 blocks of ACC_THREADS per SM at most)
+  unsigned acc_ranges;  // accumulation ranges (>= acc_threads), handed out to warps
   unsigned merge_chunk; // heads per merge thread
   unsigned log_m;       // log2 of the running-sum group
   unsigned groups;      // G = B / m groups per window
@@ -99,10 +100,11 @@ __global__ void sort_scatter_stable_kernel(const uint32_t *__restrict__ keys_in,
 // ---------------------------------------------------------------------------
 // 4. accumulation
 // ---------------------------------------------------------------------------
+// `ranges` equal ranges handed out to warps through *work (0 at launch)
 __global__ void accumulate_kernel(const uint32_t *__restrict__ keys, const uint32_t *__restrict__ vals, const affine *__restrict__ bases,
-                                  unsigned n, unsigned windows, unsigned log_b, const uint32_t *__restrict__ zeros, unsigned total_threads,
-                                  xyzz *__restrict__ buckets, uint8_t *__restrict__ flags, uint32_t *__restrict__ head_bucket,
-                                  xyzz *__restrict__ head_point);
+                                  unsigned n, unsigned windows, unsigned log_b, const uint32_t *__restrict__ zeros, unsigned ranges,
+                                  unsigned *__restrict__ work, xyzz *__restrict__ buckets, uint8_t *__restrict__ flags,
+                                  uint32_t *__restrict__ head_bucket, xyzz *__restrict__ head_point);
 
 // ---------------------------------------------------------------------------
 // 5. heads

@@ -35,7 +35,7 @@ typedef struct msm_b200_profile {
   unsigned long long nonzero_entries;  /* (window, point) pairs with a nonzero digit */
   unsigned long long nonempty_buckets; /* buckets that received at least one point */
   unsigned long long heads;            /* accumulation ranges that began inside a bucket */
-  unsigned window_bits, windows, acc_threads, launches;
+  unsigned window_bits, windows, acc_threads /* accumulation ranges */, launches;
 } msm_b200_profile;
 
 /* Same as msm_b200_execute_async, but synchronises the stream before it
