@@ -100,16 +100,21 @@ plan make_plan(unsigned n, unsigned window_bits, int sms) {
 // every chunk after the first accumulates into its own buckets, which are then
 // folded into the MSM's.  Chunk sizes grow by CHUNK_GROWTH (the pipeline takes
 // about five times as long per point as the host-to-device copy), so only the
-// first, small chunk's copy is exposed.  Reference counterpart: the chunked
-// copy/compute overlap of schedule_execution (src/msm.cu:160-334).
+// first chunk's copy is exposed; the chunk count trades that copy against
+// one bucket fold and one more pipeline start per extra chunk (cost model
+// below, in microseconds, fitted to B200 measurements: at 2^22 two chunks
+// beat three, 12.72 vs 12.90 ms end to end).  Reference counterpart: the
+// chunked copy/compute overlap of schedule_execution (src/msm.cu:160-334).
 #ifndef MSM_MAX_CHUNKS
 #define MSM_MAX_CHUNKS 4
 #endif
 #ifndef MSM_CHUNK_GROWTH
-#define MSM_CHUNK_GROWTH 4
+#define MSM_CHUNK_GROWTH 6
 #endif
 constexpr unsigned MAX_CHUNKS = MSM_MAX_CHUNKS;
 constexpr unsigned CHUNK_GROWTH = MSM_CHUNK_GROWTH;
+constexpr double COPY_US_PER_POINT = 0.58e-3; // 32 B scalar over PCIe
+constexpr double EXTRA_CHUNK_US = 360.0;      // one bucket fold + one more pipeline start
 constexpr unsigned MIN_FIRST_CHUNK = 1u << 16;
 
 struct chunking {
@@ -121,15 +126,19 @@ static chunking make_chunks(unsigned n, bool copy_inputs) {
   chunking ch;
   unsigned k = 1;
   if (copy_inputs) {
-    // largest k <= MAX_CHUNKS whose first chunk n / (1 + 4 + ... + 4^(k-1)) is >= MIN_FIRST_CHUNK
+    // the k <= MAX_CHUNKS of least modelled cost whose first chunk keeps MIN_FIRST_CHUNK points
+    double best = n * COPY_US_PER_POINT;
     unsigned long long weight = 1, total = 1;
-    while (k < MAX_CHUNKS) {
-      const unsigned long long next_total = total + weight * CHUNK_GROWTH;
-      if ((unsigned long long)n < MIN_FIRST_CHUNK * next_total)
-        break;
+    for (unsigned cand = 2; cand <= MAX_CHUNKS; cand++) {
       weight *= CHUNK_GROWTH;
-      total = next_total;
-      k++;
+      total += weight;
+      if ((unsigned long long)n < MIN_FIRST_CHUNK * total)
+        break;
+      const double cost = (double)n / total * COPY_US_PER_POINT + (cand - 1) * EXTRA_CHUNK_US;
+      if (cost < best) {
+        best = cost;
+        k = cand;
+      }
     }
   }
   ch.count = k;

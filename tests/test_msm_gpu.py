@@ -210,12 +210,13 @@ def test_events_and_callbacks(gpu, oracle):
     bc.free(bd)
 
 
-@pytest.mark.parametrize("log_n,smem,bases_on_host", [(19, "pinned", False), (20, "pageable", False), (21, "pinned", True),
-                                                     (22, "pinned", False)])
+@pytest.mark.parametrize("log_n,smem,bases_on_host", [(20, "pageable", False), (21, "pinned", True), (22, "pinned", False),
+                                                     (23, "pinned", False)])
 def test_chunked_host_inputs(gpu, oracle, log_n, smem, bases_on_host):
-    """Host-resident inputs of 2^19 points and more are processed in 2-3 chunks whose
-    copies overlap the previous chunk's work; every chunk after the first is folded
-    into the MSM's buckets.  Skewed scalars put the heavy buckets in every chunk."""
+    """Host-resident inputs of 2^20 points and more are processed in 2 chunks (3 from
+    2^23) whose copies overlap the previous chunk's work; every chunk after the
+    first is folded into the MSM's buckets.  Skewed scalars put the heavy buckets
+    in every chunk."""
     n = 1 << log_n
     scalars, k = synth.workload("skewed" if log_n % 2 else "uniform", n, 200 + log_n)
     bd, bases = generated_bases(gpu, k)
