@@ -586,21 +586,9 @@ cudaError_t enqueue_batch(const batch_plan &b, uint8_t *scratch, cudaStream_t s,
       CHECK(cudaStreamWaitEvent(fs, fork_events[0], 0));
     xyzz *gb = buckets + grp.bucket_base;
     const uint8_t *gf = flags + grp.bucket_base;
-    xyzz *tree[2] = {reinterpret_cast<xyzz *>(at(grp.tree[0])), reinterpret_cast<xyzz *>(at(grp.tree[1]))};
-    xyzz *streams[2] = {reinterpret_cast<xyzz *>(at(grp.streams[0])), reinterpret_cast<xyzz *>(at(grp.streams[1]))};
-    const unsigned group_threads = p.windows << p.log_g;
-    reduce_groups_kernel<<<(group_threads + ACC_THREADS - 1) / ACC_THREADS, ACC_THREADS, 0, fs>>>(gb, gf, p.windows, p.log_b, p.log_m, tree[0],
-                                                                                                   streams[0]);
-    CHECK(cudaGetLastError());
-    launched++;
-    for (unsigned level = 0; level < p.log_g; level++) {
-      const unsigned threads = p.windows * (level + 2) * ((1u << p.log_g) >> (level + 1));
-      const int in = level & 1;
-      reduce_level_kernel<<<(threads + ACC_THREADS - 1) / ACC_THREADS, ACC_THREADS, 0, fs>>>(tree[in], tree[in ^ 1], streams[in], streams[in ^ 1],
-                                                                                              p.windows, p.log_g, level);
-      CHECK(cudaGetLastError());
-      launched++;
-    }
+    xyzz *const tree[2] = {reinterpret_cast<xyzz *>(at(grp.tree[0])), reinterpret_cast<xyzz *>(at(grp.tree[1]))};
+    xyzz *const streams[2] = {reinterpret_cast<xyzz *>(at(grp.streams[0])), reinterpret_cast<xyzz *>(at(grp.streams[1]))};
+    CHECK(enqueue_window_sums(p, gb, gf, tree, streams, fs, launched));
     const int si = p.log_g & 1;
     const unsigned gather_threads = p.windows * RESULT_BITS;
     batch_gather_kernel<<<(gather_threads + 127) / 128, 128, 0, fs>>>(streams[si], gb, gf, reinterpret_cast<const unsigned *>(at(grp.members_dev)),

@@ -326,23 +326,29 @@ static cudaError_t enqueue_accumulation(const plan &p, const fe *scalars, const 
 }
 
 // Stage 6: bucket reduction of (buckets, flags) into the 254 results.
-static cudaError_t enqueue_reduction(const plan &p, const xyzz *buckets, const uint8_t *flags, jacobian *results, uint8_t *scratch, const layout &l,
-                                     cudaStream_t stream, stage_marks &m) {
-  xyzz *tree[2] = {reinterpret_cast<xyzz *>(scratch + l.tree[0]), reinterpret_cast<xyzz *>(scratch + l.tree[1])};
-  xyzz *streams[2] = {reinterpret_cast<xyzz *>(scratch + l.streams[0]), reinterpret_cast<xyzz *>(scratch + l.streams[1])};
+cudaError_t enqueue_window_sums(const plan &p, const xyzz *buckets, const uint8_t *flags, xyzz *const tree[2], xyzz *const streams[2],
+                                cudaStream_t stream, unsigned &launched) {
   const unsigned group_threads = p.windows << p.log_g;
   reduce_groups_kernel<<<(group_threads + ACC_THREADS - 1) / ACC_THREADS, ACC_THREADS, 0, stream>>>(buckets, flags, p.windows, p.log_b,
                                                                                                      p.log_m, tree[0], streams[0]);
   CHECK(cudaGetLastError());
-  m.launched++;
+  launched++;
   for (unsigned level = 0; level < p.log_g; level++) {
     const unsigned threads = p.windows * (level + 2) * ((1u << p.log_g) >> (level + 1));
     const int in = level & 1;
     reduce_level_kernel<<<(threads + ACC_THREADS - 1) / ACC_THREADS, ACC_THREADS, 0, stream>>>(tree[in], tree[in ^ 1], streams[in], streams[in ^ 1],
                                                                                                 p.windows, p.log_g, level);
     CHECK(cudaGetLastError());
-    m.launched++;
+    launched++;
   }
+  return cudaSuccess;
+}
+
+static cudaError_t enqueue_reduction(const plan &p, const xyzz *buckets, const uint8_t *flags, jacobian *results, uint8_t *scratch, const layout &l,
+                                     cudaStream_t stream, stage_marks &m) {
+  xyzz *const tree[2] = {reinterpret_cast<xyzz *>(scratch + l.tree[0]), reinterpret_cast<xyzz *>(scratch + l.tree[1])};
+  xyzz *const streams[2] = {reinterpret_cast<xyzz *>(scratch + l.streams[0]), reinterpret_cast<xyzz *>(scratch + l.streams[1])};
+  CHECK(enqueue_window_sums(p, buckets, flags, tree, streams, stream, m.launched));
   gather_results_kernel<<<(RESULT_BITS + 127) / 128, 128, 0, stream>>>(streams[p.log_g & 1], buckets, flags, p.windows, p.c, p.log_m, p.log_g,
                                                                        results);
   CHECK(cudaGetLastError());

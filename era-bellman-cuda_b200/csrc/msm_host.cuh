@@ -48,6 +48,13 @@ constexpr unsigned PROFILE_STAGES = 6;
 #define ACC_MIN_RANGE 256 // entries a range keeps at least when ranges are multiplied
 #endif
 
+// Per-window sums of the reduction (reduce_groups_kernel, then one
+// reduce_level_kernel per level) for the p.windows windows of 2^(c-1) bucket
+// slots at `buckets`; afterwards streams[p.log_g & 1] holds each window's sums
+// for the gather kernels.  tree / streams: the ping-pong buffers of the plan.
+cudaError_t enqueue_window_sums(const plan &p, const xyzz *buckets, const uint8_t *flags, xyzz *const tree[2], xyzz *const streams[2],
+                                cudaStream_t stream, unsigned &launched);
+
 unsigned default_window_bits(unsigned long long n);
 unsigned accumulation_ranges(unsigned threads, unsigned long long entries, unsigned per_thread);
 plan make_plan(unsigned n, unsigned window_bits, int sms);
