@@ -528,6 +528,17 @@ def main():
         line["roofline_hbm"] = {"kernels": "digits + sort", "achieved": round(sort_bytes / sort_s / 1e9, 1), "peak": hbm, "unit": "GB/s",
                                 "frac": round(sort_bytes / sort_s / 1e9 / hbm, 4), "peak_source": hbm_src,
                                 "bytes": "32 B scalar + 8 B/entry digit write; 20 B/entry per radix pass (4 histogram + 8 read + 8 write)"}
+        # ---- the optional on-device final reduction of the 254 results ---------
+        point_dev = bc.malloc(80)  # sizeof(msm_b200_affine_point)
+
+        def step_final_sum():
+            bc.check(bc.final_sum_async(results_dev, point_dev, stream), "msm_b200_final_sum_async")
+
+        step_final_sum()
+        line["final_sum"] = {"ms": round(time_steps(bc, stream, args.steps, step_final_sum), 4),
+                             "what": "msm_b200_final_sum_async: sum 2^i R_i of the 254 results as one canonical affine point, on "
+                                     "the device (one block; latency-bound: 255 dependent doublings, 8 additions, one inversion)"}
+        bc.free(point_dev)
         if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(bc, scalars, bases_dev)
     if dist.rank == 0 and dist.world == 1 and not args.no_batched:

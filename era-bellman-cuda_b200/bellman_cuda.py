@@ -104,6 +104,20 @@ class MsmB200Profile(ctypes.Structure):
         return self.nonzero_entries - self.nonempty_buckets - self.heads
 
 
+class AffinePoint(ctypes.Structure):
+    """msm_b200_affine_point (include/bellman-cuda-b200.h): standard-form,
+    fully reduced x and y, infinity flag."""
+
+    _fields_ = [("x", ctypes.c_uint32 * 8), ("y", ctypes.c_uint32 * 8), ("infinity", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32 * 3)]
+
+    def as_tuple(self):
+        """(infinity, x, y) with x, y as Python integers."""
+        x = sum(int(v) << (32 * i) for i, v in enumerate(self.x))
+        y = sum(int(v) << (32 * i) for i, v in enumerate(self.y))
+        return (bool(self.infinity), x, y)
+
+
 class RequestTimes(ctypes.Structure):
     """msm_b200_request_times (include/bellman-cuda-b200.h)."""
 
@@ -190,6 +204,7 @@ class BellmanCuda:
                                                   ctypes.POINTER(ctypes.c_uint)],
                 "msm_b200_measure_mul_throughput": [u, ctypes.POINTER(ctypes.c_double)],
                 "msm_b200_execute_no_alloc_async": [Handle, vp, vp, vp, u],
+                "msm_b200_final_sum_async": [vp, vp, Handle],
                 "msm_b200_base_table_create": [ctypes.POINTER(vp), vp, u, ctypes.POINTER(u), u, Handle],
                 "msm_b200_base_table_bytes": [vp, ctypes.POINTER(sz)],
                 "msm_b200_base_table_destroy": [vp],
@@ -394,6 +409,12 @@ class BellmanCuda:
     def msm_no_alloc(self, stream: Handle, bases, scalars, results, count: int) -> int:
         """msm_b200_execute_no_alloc_async: device buffers only, count <= NO_ALLOC_MAX_COUNT; returns the bc_error."""
         return self.lib.msm_b200_execute_no_alloc_async(stream, _ptr(bases), _ptr(scalars), _ptr(results), count)
+
+    def final_sum_async(self, results, point, stream: Handle) -> int:
+        """msm_b200_final_sum_async: sum 2^i R_i of 254 Jacobian results (device or
+        pinned memory) into one msm_b200_affine_point at `point` (device or pinned
+        memory); returns the bc_error."""
+        return self.lib.msm_b200_final_sum_async(_ptr(results), _ptr(point), stream)
 
     # -- batched MSMs over a resident base table -------------------------------
     def base_table_create(self, bases, count: int, stream: Handle, window_bits=None) -> int:

@@ -174,6 +174,32 @@ struct curve {
     return r;
   }
 
+  // Jacobian (X, Y, Z; x = X/Z^2, y = Y/Z^3) -> XYZZ (X, Y, Z^2, Z^3); the
+  // Jacobian infinity (Z = 0) gives ZZ = 0, the XYZZ infinity.
+  static BN_HD xyzz from_jacobian(const jacobian &p) {
+    xyzz r;
+    r.x = p.x;
+    r.y = p.y;
+    r.zz = fq::sqr(p.z);
+    r.zzz = fq::mul(r.zz, p.z);
+    return r;
+  }
+
+  // Canonical affine output: x and y in standard (not Montgomery) form,
+  // fully reduced; true, with x = y = 0, for infinity.  One binary inversion
+  // of ZZ ZZZ gives 1/ZZ = ZZZ / (ZZ ZZZ) and 1/ZZZ = ZZ / (ZZ ZZZ).
+  static BN_HD_COLD bool to_affine_standard(const xyzz &p, fe &x, fe &y) {
+    if (is_inf(p)) {
+      x = fq::zero();
+      y = fq::zero();
+      return true;
+    }
+    const fe inv = fq::to_mont(fq::inverse_binary(fq::from_mont(fq::mul(p.zz, p.zzz))));
+    x = fq::from_mont(fq::mul(p.x, fq::mul(p.zzz, inv)));
+    y = fq::from_mont(fq::mul(p.y, fq::mul(p.zz, inv)));
+    return false;
+  }
+
   // XYZZ -> affine for a finite p: one inversion of ZZ ZZZ gives both
   // 1/ZZ = ZZZ / (ZZ ZZZ) and 1/ZZZ = ZZ / (ZZ ZZZ).  Output fully reduced.
   static BN_HD_COLD affine to_affine(const xyzz &p) {

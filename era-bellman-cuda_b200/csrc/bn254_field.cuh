@@ -845,6 +845,101 @@ template <class F> struct field {
     return cc::subc(0, 0) != 0;
   }
 
+  // ---- binary inversion (standard form) ------------------------------------
+  static BN_HD bool is_one_raw(const fe &a) {
+    uint32_t acc = a.l[0] ^ 1u;
+#pragma unroll
+    for (int i = 1; i < 8; i++)
+      acc |= a.l[i];
+    return acc == 0;
+  }
+
+  static BN_HD fe shr1(const fe &a, uint32_t top) {
+    fe r;
+#pragma unroll
+    for (int i = 0; i < 7; i++)
+      r.l[i] = (a.l[i] >> 1) | (a.l[i + 1] << 31);
+    r.l[7] = (a.l[7] >> 1) | (top << 31);
+    return r;
+  }
+
+  // a / 2 mod m for a canonical a: a >> 1, or (a + m) >> 1 for odd a (the
+  // carry of a + m becomes bit 255)
+  static BN_HD fe half_mod(const fe &a) {
+    if (!(a.l[0] & 1))
+      return shr1(a, 0);
+    fe s;
+    s.l[0] = cc::add_cc(a.l[0], F::mod(0));
+#pragma unroll
+    for (int i = 1; i < 8; i++)
+      s.l[i] = cc::addc_cc(a.l[i], F::mod(i));
+    return shr1(s, cc::addc(0, 0));
+  }
+
+  // a - b for a >= b
+  static BN_HD fe sub_raw(const fe &a, const fe &b) {
+    fe d;
+    d.l[0] = cc::sub_cc(a.l[0], b.l[0]);
+#pragma unroll
+    for (int i = 1; i < 7; i++)
+      d.l[i] = cc::subc_cc(a.l[i], b.l[i]);
+    d.l[7] = cc::subc(a.l[7], b.l[7]);
+    return d;
+  }
+
+  // a - b mod m for canonical a, b
+  static BN_HD fe sub_canonical(const fe &a, const fe &b) {
+    if (!lt(a, b))
+      return sub_raw(a, b);
+    fe s;
+    s.l[0] = cc::add_cc(a.l[0], F::mod(0));
+#pragma unroll
+    for (int i = 1; i < 7; i++)
+      s.l[i] = cc::addc_cc(a.l[i], F::mod(i));
+    s.l[7] = cc::addc(a.l[7], F::mod(7));
+    return sub_raw(s, b); // a + m - b < m, no wrap
+  }
+
+  // a^-1 mod m for a canonical a in standard (not Montgomery) form, by the
+  // binary extended Euclidean algorithm (Hankerson, Menezes and Vanstone,
+  // "Guide to Elliptic Curve Cryptography", Algorithm 2.22): with u = x1 a
+  // and v = x2 a (mod m) kept invariant, halvings of the even one and the
+  // subtraction of the smaller from the larger bring u or v to 1.  About
+  // 2 x 254 rounds of shifts and subtractions: a much shorter dependent chain
+  // than the 254 Montgomery squarings of the Fermat inverse, which is what a
+  // single GPU thread finishing an MSM needs.  0 (and any a sharing a factor
+  // with m) gives 0; every loop is bounded.
+  static BN_HD fe inverse_binary(const fe &a) {
+    fe u = a, v = modulus(), x1 = zero(), x2 = zero();
+    x1.l[0] = 1;
+    if (is_zero_exact(a))
+      return zero();
+    for (int round = 0; round < 1024; round++) {
+      if (is_one_raw(u))
+        return x1;
+      if (is_one_raw(v))
+        return x2;
+      if (is_zero_exact(u) || is_zero_exact(v))
+        break;
+      while (!(u.l[0] & 1)) {
+        u = shr1(u, 0);
+        x1 = half_mod(x1);
+      }
+      while (!(v.l[0] & 1)) {
+        v = shr1(v, 0);
+        x2 = half_mod(x2);
+      }
+      if (!lt(u, v)) {
+        u = sub_raw(u, v);
+        x1 = sub_canonical(x1, x2);
+      } else {
+        v = sub_raw(v, u);
+        x2 = sub_canonical(x2, x1);
+      }
+    }
+    return zero();
+  }
+
   // exponentiation by m - 2 (Fermat inverse), Montgomery domain; 0 -> 0
   static BN_HD fe inverse(const fe &a) {
     fe e = modulus();

@@ -6,6 +6,7 @@
 #pragma once
 
 #include "bellman-cuda.h"
+#include <stdint.h>
 
 #ifdef __cplusplus
 extern "C" {
@@ -193,6 +194,31 @@ bc_error msm_b200_server_destroy(msm_b200_server server);
 #define MSM_B200_NO_ALLOC_MAX_COUNT 65536u
 #define MSM_B200_NO_ALLOC_SCRATCH_BYTES (64u << 20)
 bc_error msm_b200_execute_no_alloc_async(bc_stream stream, const void *bases, const void *scalars, void *results, unsigned count);
+
+/* The caller-side final reduction on the GPU (no counterpart in the
+ * reference, whose callers run it on the host: src/bellman-cuda.h:496-505).
+ *
+ * Writes sum over i < 254 of 2^i R_i of the 254 Jacobian points at `results`
+ * (the layout msm_execute_async writes: Montgomery-form Fq coordinates below
+ * 2p, x = X/Z^2, y = Y/Z^3, Z = 0 for infinity; this library's results and
+ * the reference's both qualify) to `point` as one canonical affine point:
+ * x and y in standard (not Montgomery) form, fully reduced mod p, 8
+ * little-endian 32-bit limbs each; infinity = 1 and x = y = 0 for the point
+ * at infinity.  The bytes therefore compare equal for equal points, whatever
+ * window split produced the R_i.
+ *
+ * `results` (16-byte aligned) and `point` must be device memory or pinned
+ * host memory (registered or cudaMallocHost'd; the kernel reads and writes it
+ * in place); a null or pageable pointer returns bc_error_invalid_value before
+ * anything is enqueued.  Asynchronous on `stream`, one kernel of one block,
+ * no allocation.  Enqueue it after the MSM on the same stream. */
+typedef struct msm_b200_affine_point {
+  uint32_t x[8];
+  uint32_t y[8];
+  uint32_t infinity;
+  uint32_t reserved[3];
+} msm_b200_affine_point;
+bc_error msm_b200_final_sum_async(const void *results, msm_b200_affine_point *point, bc_stream stream);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

@@ -33,6 +33,7 @@ void fc_fq_op(int op, const uint32_t *a, const uint32_t *b, uint32_t *out, int n
     case 8: r = fq::inverse(x); break;
     case 9: r = fq::dbl(x); break;
     case 10: r = fq::neg_nonzero(x); break;
+    case 11: r = fq::inverse_binary(x); break;
     }
     st(out + 8 * i, r);
   }
@@ -86,6 +87,14 @@ void fc_add(const uint32_t *p, const uint32_t *q, uint32_t *out) { st(out, curve
 void fc_dbl(const uint32_t *p, uint32_t *out) { st(out, curve::dbl(ld<xyzz>(p))); }
 void fc_from_affine(const uint32_t *a, uint32_t *out) { st(out, curve::from_affine(ld<affine>(a))); }
 void fc_to_jacobian(const uint32_t *p, uint32_t *out) { st(out, curve::to_jacobian(ld<xyzz>(p))); }
+void fc_from_jacobian(const uint32_t *p, uint32_t *out) { st(out, curve::from_jacobian(ld<jacobian>(p))); }
+int fc_to_affine_standard(const uint32_t *p, uint32_t *out) {
+  fe x, y;
+  const bool inf = curve::to_affine_standard(ld<xyzz>(p), x, y);
+  st(out, x);
+  st(out + 8, y);
+  return inf ? 1 : 0;
+}
 void fc_infinity(uint32_t *out) { st(out, curve::infinity()); }
 
 } // extern "C"

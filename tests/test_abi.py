@@ -91,3 +91,27 @@ def test_reference_build_exports_same_msm_surface():
     ref_syms = set(line.split()[-1] for line in out.splitlines())
     mine = set(declared_functions())
     assert {n for n in mine if not n.startswith("msm_b200_") and n != "ff_tear_down"} <= ref_syms
+
+
+POINT_PROGRAM = r"""
+#include <stdio.h>
+#include <stddef.h>
+#include "bellman-cuda-b200.h"
+int main(void) {
+  printf("%zu %zu %zu %zu\n", sizeof(msm_b200_affine_point), offsetof(msm_b200_affine_point, y),
+         offsetof(msm_b200_affine_point, infinity), offsetof(msm_b200_affine_point, reserved));
+  return 0;
+}
+"""
+
+
+def test_affine_point_layout_matches_ctypes(tmp_path):
+    """msm_b200_affine_point, the final sum's output, as C lays it out."""
+    import bellman_cuda as bc
+    src = tmp_path / "point.c"
+    exe = tmp_path / "point"
+    src.write_text(POINT_PROGRAM)
+    subprocess.run(["gcc", "-std=c11", "-I", INCLUDE, str(src), "-o", str(exe)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    A = bc.AffinePoint
+    assert got == [ctypes.sizeof(A), A.y.offset, A.infinity.offset, A.reserved.offset] == [80, 32, 64, 68]

@@ -80,6 +80,19 @@ def test_fq_inverse(field_check):
         assert (r * x * RINV) % P == (1 << 256) % P
 
 
+def test_fq_inverse_binary(field_check):
+    """Binary extended-Euclid inverse of canonical standard-form values
+    (the on-device final reduction's inversion): a * a^-1 = 1 mod p, 0 -> 0."""
+    rng = np.random.Generator(np.random.PCG64(12))
+    xs = [int.from_bytes(rng.bytes(32), "little") % P for _ in range(2000)]
+    xs += [0, 1, 2, 3, P - 1, P - 2, P // 2, (P + 1) // 2, 1 << 128, (1 << 253) - 1, 0xFFFFFFFF, 1 << 32]
+    a = arr(xs)
+    out = np.zeros_like(a)
+    field_check.fc_fq_op(11, ptr(a), ptr(a), ptr(out), len(xs))
+    for x, r in zip(xs, ints(out)):
+        assert r == (pow(x, -1, P) if x else 0), hex(x)
+
+
 def test_fq_mul_sub_mul(field_check, pairs):
     xs, ys = pairs
     rng = np.random.Generator(np.random.PCG64(5))
@@ -192,3 +205,27 @@ def test_karatsuba_montgomery_matches_cios(field_check, pairs):
     for x, y, c_, k_ in zip(xs, ys, ints(out_c), ints(out_k)):
         assert c_ < 2 * P and k_ < 2 * P
         assert c_ % P == k_ % P == x * y * RINV % P
+
+
+def test_jacobian_round_trip_and_standard_affine(field_check, oracle):
+    """from_jacobian / to_affine_standard (the final-sum kernel's input and
+    output conversions): Jacobian points with random Z, infinity with Z = 0."""
+    table = H.load_g_bases()
+    f = field_check
+    rng = np.random.Generator(np.random.PCG64(13))
+    for i in (0, 3, 17, 100, 255):
+        x, y = table[i]
+        z = int.from_bytes(rng.bytes(32), "little") % P or 1
+        jac = arr([x * z * z % P * (1 << 256) % P, y * z ** 3 % P * (1 << 256) % P, z * (1 << 256) % P])
+        p = np.zeros(32, np.uint32)
+        f.fc_from_jacobian(ptr(jac), ptr(p))
+        assert xyzz_to_affine(p) == (False, x, y)
+        out = np.zeros(16, np.uint32)
+        assert f.fc_to_affine_standard(ptr(p), ptr(out)) == 0
+        assert (H.to_int(out[:8]), H.to_int(out[8:])) == (x, y)
+    inf_jac = arr([0, (1 << 256) % P, 0])  # the reference encoding (0, 1, 0)
+    p = np.zeros(32, np.uint32)
+    f.fc_from_jacobian(ptr(inf_jac), ptr(p))
+    out = np.ones(16, np.uint32)
+    assert f.fc_to_affine_standard(ptr(p), ptr(out)) == 1
+    assert not out.any()
