@@ -154,6 +154,45 @@ template <int KIND> __global__ void __launch_bounds__(128) component_kernel(uint
   sink[tid] = x.l[0] ^ z.l[1] ^ acc;
 }
 
+// kind 10: sixteen independent double-precision FMAs per iteration (the
+// FP64 pipe, a second multiplier beside the integer one); kind 11: the
+// sixteen mad.lo / mad.hi of kind 0 and sixteen FMAs interleaved, counting
+// only the integer multiplies, to see whether the two pipes overlap.
+template <bool MIXED> __global__ void __launch_bounds__(256) dfma_kernel(uint32_t seed, unsigned iters, uint32_t *sink) {
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+  double d[16];
+  const double m = 0.999 + 1e-9 * (seed & 7), c = 0.5 + 1e-9 * (tid & 15);
+#pragma unroll
+  for (int j = 0; j < 16; j++)
+    d[j] = 1.0 + j + 1e-6 * tid;
+  uint32_t lo[8], hi[8];
+  const uint32_t b = seed ^ (tid * 0x9e3779b9u), cc_ = seed + tid;
+#pragma unroll
+  for (int j = 0; j < 8; j++) {
+    lo[j] = tid * (j + 3);
+    hi[j] = tid ^ (j * 0x85ebca6bu);
+  }
+  for (unsigned i = 0; i < iters; i++) {
+#pragma unroll
+    for (int j = 0; j < 16; j++) {
+      d[j] = __fma_rn(d[j], m, c);
+      if (MIXED && (j & 1) == 0) {
+        asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(lo[j / 2]) : "r"(b), "r"(cc_));
+        asm volatile("mad.hi.u32 %0, %0, %1, %2;" : "+r"(hi[j / 2]) : "r"(b), "r"(cc_));
+      }
+    }
+  }
+  double x = 0;
+  uint32_t y = 0;
+#pragma unroll
+  for (int j = 0; j < 16; j++)
+    x += d[j];
+#pragma unroll
+  for (int j = 0; j < 8; j++)
+    y ^= lo[j] ^ hi[j];
+  sink[tid] = (uint32_t)(long long)x ^ y;
+}
+
 // kind 3: XYZZ += affine chain (never the doubling branch: acc = k*G, k >= 2)
 __global__ void __launch_bounds__(128) madd_kernel(unsigned iters, uint32_t *sink) {
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -174,7 +213,7 @@ __global__ void __launch_bounds__(128) madd_kernel(unsigned iters, uint32_t *sin
 } // namespace
 
 extern "C" bc_error msm_b200_measure_mul_throughput(unsigned kind, double *mulops_per_second) {
-  if (!mulops_per_second || kind > 9)
+  if (!mulops_per_second || kind > 11)
     return bc_error_invalid_value;
   int device = 0, sms = 0;
   cudaError_t e = cudaGetDevice(&device);
@@ -182,7 +221,7 @@ extern "C" bc_error msm_b200_measure_mul_throughput(unsigned kind, double *mulop
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   if (e != cudaSuccess)
     return static_cast<bc_error>(e);
-  const bool light = kind < 2 || kind == 4 || kind == 5;
+  const bool light = kind < 2 || kind == 4 || kind == 5 || kind == 10 || kind == 11;
   const unsigned threads = light ? 256 : 128;
   const unsigned blocks = light ? sms * 8 : sms * 4;
   const unsigned iters = light ? 65536 : kind == 2 ? 4096 : kind == 3 ? 1024 : kind == 9 ? 65536 : 4096;
@@ -217,6 +256,8 @@ extern "C" bc_error msm_b200_measure_mul_throughput(unsigned kind, double *mulop
       case 7: component_kernel<7><<<blocks, threads, 0, stream>>>(0x1234567u, iters, sink); break;
       case 8: component_kernel<8><<<blocks, threads, 0, stream>>>(0x1234567u, iters, sink); break;
       case 9: component_kernel<9><<<blocks, threads, 0, stream>>>(0x1234567u, iters, sink); break;
+      case 10: dfma_kernel<false><<<blocks, threads, 0, stream>>>(0x1234567u, iters, sink); break;
+      case 11: dfma_kernel<true><<<blocks, threads, 0, stream>>>(0x1234567u, iters, sink); break;
       default: madd_kernel<<<blocks, threads, 0, stream>>>(iters, sink); break;
       }
       if ((e = cudaGetLastError()) != cudaSuccess)

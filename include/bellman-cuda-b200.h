@@ -59,6 +59,10 @@ bc_error msm_b200_execute_staged_async(const msm_b200_configuration *configurati
  *   kind 4: independent mad.lo only;  kind 5: independent mad.hi only
  *   kinds 6..9: squaring, a*b - c*d, 512-bit products, add/sub pairs (the
  *   last reports field additions per second, not multiply instructions)
+ *   kind 10: independent double-precision FMAs (FMAs per second)
+ *   kind 11: kind 0's integer multiplies interleaved with as many FMAs
+ *   (integer multiply instructions per second: equal to kind 0 when the
+ *   FP64 pipe runs beside the integer one)
  * Synchronous; about 0.1 s. */
 bc_error msm_b200_measure_mul_throughput(unsigned kind, double *mulops_per_second);
 
