@@ -114,11 +114,22 @@ __global__ void __launch_bounds__(256) batch_digits_kernel(const batch_instance 
   const unsigned k = lo, i = g - s_off[k];
   const batch_instance d = inst[k];
   const fe *scalars = io[k].scalars;
-  scalar_digits(load_fe_streaming(scalars + i), d.c, d.windows, [&](unsigned w, uint32_t magnitude, uint32_t negative) {
-    const size_t out = d.entry_offset + (size_t)w * d.n + i;
-    keys[out] = digit_key(magnitude);
-    vals[out] = (w * d.stride + i) | (negative << 31);
-  });
+  const fe scalar = load_fe_streaming(scalars + i);
+  auto digits = [&](auto width) {
+    scalar_digits_fixed<decltype(width)::value>(scalar, d.c, d.windows, [&](unsigned w, uint32_t magnitude, uint32_t negative) {
+      const size_t out = d.entry_offset + (size_t)w * d.n + i;
+      keys[out] = digit_key(magnitude);
+      vals[out] = (w * d.stride + i) | (negative << 31);
+    });
+  };
+  // the widths the batch table picks for its large instances get unrolled code
+  switch (d.c) {
+  case 16: digits(width_constant<16>{}); break;
+  case 17: digits(width_constant<17>{}); break;
+  case 20: digits(width_constant<20>{}); break;
+  case 22: digits(width_constant<22>{}); break;
+  default: digits(width_constant<0>{}); break;
+  }
 }
 
 // The first pass drops zero digits (counted into zeros[k], which must start at

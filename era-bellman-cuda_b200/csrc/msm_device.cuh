@@ -74,7 +74,13 @@ __device__ __forceinline__ uint32_t limb_at(const fe &s, unsigned k) {
 // 1. digits
 // ---------------------------------------------------------------------------
 // Signed windows of one scalar; emit(w, key, negative) for each window.
-template <class EMIT> __device__ __forceinline__ void scalar_digits(const fe &scalar_mont, unsigned c, unsigned windows, EMIT emit) {
+// C != 0 fixes the window width at compile time (windows = ceil(254 / C)):
+// the window loop unrolls and every limb index is a constant, which removes
+// the run-time limb selection; C == 0 takes c and windows at run time.
+template <unsigned C, class EMIT>
+__device__ __forceinline__ void scalar_digits_fixed(const fe &scalar_mont, unsigned c_run, unsigned windows_run, EMIT emit) {
+  const unsigned c = C ? C : c_run;
+  const unsigned windows = C ? (RESULT_BITS + C - 1) / C : windows_run;
   fe s = fr::from_mont(scalar_mont); // canonical, < r
   // r - s (s == 0 gives r, which is never the smaller one)
   const fe m = fr::modulus();
@@ -89,6 +95,7 @@ template <class EMIT> __device__ __forceinline__ void scalar_digits(const fe &sc
   const uint32_t half = 1u << (c - 1);
   const uint32_t mask = (1u << c) - 1;
   uint32_t carry = 0;
+#pragma unroll
   for (unsigned w = 0; w < windows; w++) {
     const unsigned bit = w * c;
     const unsigned limb = bit >> 5;
@@ -106,6 +113,15 @@ template <class EMIT> __device__ __forceinline__ void scalar_digits(const fe &sc
     emit(w, raw, negative ^ (flip ? 1u : 0u));
   }
 }
+
+template <class EMIT> __device__ __forceinline__ void scalar_digits(const fe &scalar_mont, unsigned c, unsigned windows, EMIT emit) {
+  scalar_digits_fixed<0>(scalar_mont, c, windows, emit);
+}
+
+// a compile-time window width passed to generic lambdas
+template <unsigned C> struct width_constant {
+  static constexpr unsigned value = C;
+};
 
 // Sort key of a signed digit of magnitude m = |d| in [0, 2^(c-1)]: m - 1, so
 // the keys of nonzero digits take c - 1 bits, and a zero digit wraps to

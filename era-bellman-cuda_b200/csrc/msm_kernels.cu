@@ -29,16 +29,27 @@ __global__ void __launch_bounds__(SORT_THREADS) digits_histogram_kernel(const fe
   for (unsigned k = threadIdx.x; k < windows * (SORT_RADIX + 1); k += blockDim.x)
     hist[k] = 0;
   __syncthreads();
-  for (unsigned k = 0; k < SORT_ITEMS; k++) {
-    const unsigned i = tile * SORT_TILE + k * SORT_THREADS + threadIdx.x;
-    if (i < n)
-      scalar_digits(load_fe_streaming(scalars + i), c, windows, [&](unsigned w, uint32_t magnitude, uint32_t negative) {
-        const size_t out = (size_t)w * n + i;
-        const uint32_t key = digit_key(magnitude);
-        keys[out] = key;
-        vals[out] = i | (negative << 31);
-        atomicAdd(magnitude ? &hist[w * SORT_RADIX + (key & (SORT_RADIX - 1))] : &zero_digits[w], 1u);
-      });
+  auto tile_digits = [&](auto width) {
+    constexpr unsigned C = decltype(width)::value;
+    for (unsigned k = 0; k < SORT_ITEMS; k++) {
+      const unsigned i = tile * SORT_TILE + k * SORT_THREADS + threadIdx.x;
+      if (i < n)
+        scalar_digits_fixed<C>(load_fe_streaming(scalars + i), c, windows, [&](unsigned w, uint32_t magnitude, uint32_t negative) {
+          const size_t out = (size_t)w * n + i;
+          const uint32_t key = digit_key(magnitude);
+          keys[out] = key;
+          vals[out] = i | (negative << 31);
+          atomicAdd(magnitude ? &hist[w * SORT_RADIX + (key & (SORT_RADIX - 1))] : &zero_digits[w], 1u);
+        });
+    }
+  };
+  // the widths the size tables pick from 2^15 points on get unrolled code
+  switch (c) {
+  case 13: tile_digits(width_constant<13>{}); break;
+  case 15: tile_digits(width_constant<15>{}); break;
+  case 16: tile_digits(width_constant<16>{}); break;
+  case 17: tile_digits(width_constant<17>{}); break;
+  default: tile_digits(width_constant<0>{}); break;
   }
   __syncthreads();
   for (unsigned k = threadIdx.x; k < windows * SORT_RADIX; k += blockDim.x)
