@@ -195,12 +195,20 @@ def time_steps(bc, stream, k: int, enqueue) -> float:
     return ms
 
 
-def cpu_baseline(bc, scalars_all: np.ndarray, bases_dev: int, target_s: float = 6.0):
-    """Multithreaded host Pippenger (the CPU oracle) on a bounded prefix of the workload."""
+def cpu_baseline(bc, scalars_all: np.ndarray, bases_dev: int, results_dev: int, target_s: float = 6.0):
+    """Multithreaded host Pippenger (the CPU oracle) on a bounded prefix of the
+    workload; also the caller-side Horner pass over this run's 254 results on
+    one host core, the CPU counterpart of msm_b200_final_sum_async."""
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import oracle as orc
     subprocess.run(["make", "-s", "-C", os.path.join(REPO, "oracle")], check=True)
     o = orc.Oracle()
+    results = bc.from_device(results_dev, (254, 24))
+    horner_s = []
+    for _ in range(5):
+        t0 = time.perf_counter()
+        o.horner(results)
+        horner_s.append(time.perf_counter() - t0)
     cores = os.cpu_count() or 1
     n = 1 << 14
     best = None
@@ -214,7 +222,8 @@ def cpu_baseline(bc, scalars_all: np.ndarray, bases_dev: int, target_s: float = 
     n, secs = best
     return {"value": n / secs / 1e6, "unit": "Mpoints/s", "cores": cores, "kind": "port",
             "sample": f"host Pippenger (oracle/bn254_oracle.c, {cores} threads) over the first 2^{n.bit_length() - 1} points of the same "
-                      f"workload, {secs:.2f} s wall"}
+                      f"workload, {secs:.2f} s wall",
+            "host_horner_ms": round(1e3 * statistics.median(horner_s), 4)}
 
 
 def generated_table(bc, seed: int, n: int, stream) -> int:
@@ -540,7 +549,7 @@ def main():
                                      "the device (one block; latency-bound: 255 dependent doublings, 8 additions, one inversion)"}
         bc.free(point_dev)
         if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(bc, scalars, bases_dev)
+            line["cpu_baseline"] = cpu_baseline(bc, scalars, bases_dev, results_dev)
     if dist.rank == 0 and dist.world == 1 and not args.no_batched:
         line["batched"] = batched_section(ours, bc, pool, stream, max(3, args.steps // 2), 2)
     if dist.rank == 0 and dist.world == 1 and not args.no_serving and args.impl == "b200":

@@ -5,13 +5,14 @@
 // (src/bellman-cuda.h:496-505; tests/msm_test.cu:116-126).
 //
 // Whatever the order of the additions, the term 2^253 R_253 needs 253
-// dependent doublings, so the sum is latency-bound on one thread.  A Horner
-// pass also puts 253 additions on that chain; a pairwise tree over the bits
-// puts 8: thread t starts from R_2t + 2 R_2t+1, and at level L = 1..7 the
-// threads with t mod 2^L = 0 add their partner t + 2^(L-1), doubled 2^L
-// times (its lowest bit is 2^L above theirs).  Critical path: 255 doublings
-// and 8 additions, then one inversion by the binary extended Euclidean
-// algorithm (far shorter than a Fermat inverse's 254 squarings).
+// dependent doublings, so the sum is latency-bound.  A Horner pass also puts
+// 253 additions on that chain; a pairwise tree over the bits puts 8: thread t
+// starts from R_2t + 2 R_2t+1, and at level L = 1..7 the sum starting at bit
+// 2t (t mod 2^L = 0) takes its partner's (t + 2^(L-1)), doubled 2^L times.
+// From level 2 on (252 of the 255 doublings on the critical path) each
+// doubling is shared by four lanes (dbl_group4).  Then one inversion by the
+// binary extended Euclidean algorithm (far shorter than a Fermat inverse's
+// 254 squarings).
 #include "bellman-cuda-b200.h"
 #include "msm_device.cuh"
 
@@ -21,31 +22,85 @@ namespace msm_b200 {
 
 constexpr unsigned FINAL_THREADS = 128; // threads t < 127 start from results 2t, 2t + 1
 
+__device__ __forceinline__ fe shfl_fe(const fe &v, unsigned src) {
+  fe r;
+#pragma unroll
+  for (int k = 0; k < 8; k++)
+    r.l[k] = __shfl_sync(0xffffffffu, v.l[k], src);
+  return r;
+}
+
+__device__ __forceinline__ fe select_fe(bool c, const fe &a, const fe &b) {
+  fe r;
+#pragma unroll
+  for (int k = 0; k < 8; k++)
+    r.l[k] = c ? a.l[k] : b.l[k];
+  return r;
+}
+
+// One XYZZ doubling (dbl-2008-s-1, the formula of curve::dbl) by a group of
+// four lanes: lanes 4g..4g+3 hold the same point and all return its double.
+// The formula's independent products run on different lanes of the group in
+// three rounds -- X^2 | (2Y)^2;  M^2 | X V | U V | V ZZ;  M (S - X3) - W Y |
+// W ZZZ -- and shuffles share the results, so one doubling costs three
+// dependent products instead of ten.  Every lane runs the same instructions
+// on its own operands (no divergence), so every lane of the warp must call
+// it.  Infinity (ZZ = 0) maps to a point with ZZ = 0, i.e. to infinity.
+__device__ __forceinline__ xyzz dbl_group4(const xyzz &p) {
+  const unsigned lane = threadIdx.x & 31, role = lane & 3, base = lane & ~3u;
+  const fe U = fq::dbl(p.y);
+  const fe r1 = fq::sqr(select_fe(role == 0, p.x, U));
+  const fe X2 = shfl_fe(r1, base), V = shfl_fe(r1, base + 1);
+  const fe M = fq::add(fq::dbl(X2), X2);
+  const fe a2 = role == 0 ? M : role == 1 ? p.x : role == 2 ? U : V;
+  const fe b2 = role == 0 ? M : role == 3 ? p.zz : V;
+  const fe r2 = fq::mul(a2, b2);
+  const fe M2 = shfl_fe(r2, base), S = shfl_fe(r2, base + 1), W = shfl_fe(r2, base + 2), ZZ3 = shfl_fe(r2, base + 3);
+  xyzz r;
+  r.x = fq::sub(M2, fq::dbl(S));
+  const bool lead = role == 0;
+  const fe r3 = fq::mul_sub_mul(lead ? M : W, lead ? fq::sub(S, r.x) : p.zzz, lead ? W : fq::zero(), lead ? p.y : fq::zero());
+  r.y = shfl_fe(r3, base);
+  r.zzz = shfl_fe(r3, base + 1);
+  r.zz = ZZ3;
+  return r;
+}
+
 __global__ void __launch_bounds__(FINAL_THREADS) final_sum_kernel(const jacobian *__restrict__ results, msm_b200_affine_point *point) {
-  __shared__ xyzz partner[FINAL_THREADS];
+  __shared__ xyzz part[FINAL_THREADS]; // part[t]: the sum of the bits starting at 2t (weights relative to 2^2t)
   const unsigned t = threadIdx.x;
+  // level 0, one thread per pair of results
   xyzz q = curve::infinity();
   if (2 * t + 1 < RESULT_BITS) {
     const xyzz lo = curve::from_jacobian(results[2 * t]);
     const xyzz hi = curve::from_jacobian(results[2 * t + 1]);
     q = curve::add(lo, curve::dbl(hi));
   }
-  for (unsigned level = 1; (1u << level) <= FINAL_THREADS; level++) {
-    const unsigned half = 1u << (level - 1), mask = 2 * half - 1;
-    if ((t & mask) == half)
-      partner[t] = q;
-    __syncthreads();
-    if ((t & mask) == 0) {
-      xyzz o = partner[t + half]; // t + half <= FINAL_THREADS - half
+  part[t] = q;
+  __syncthreads();
+  // level 1, one thread per pair of level-0 sums (reads odd entries, writes even ones)
+  if ((t & 1) == 0)
+    part[t] = curve::add(part[t], curve::dbl(curve::dbl(part[t + 1])));
+  __syncthreads();
+  // levels 2..7: group g of four lanes adds part[g 2^L + 2^(L-1)], doubled
+  // 2^L times, into part[g 2^L]; groups past the last pair (and whole warps
+  // without an active group) double a copy of part[0] and write nothing
+  for (unsigned level = 2; (1u << level) <= FINAL_THREADS; level++) {
+    const unsigned pairs = FINAL_THREADS >> level, group = t >> 2;
+    const unsigned target = group << level, partner = target + (1u << (level - 1));
+    if (((t & ~31u) >> 2) < pairs) { // warp-uniform: the warp's first group is active
+      const bool active = group < pairs;
+      xyzz o = part[active ? partner : 0];
       for (unsigned k = 0; k < (1u << level); k++)
-        o = curve::dbl(o);
-      q = curve::add(q, o);
+        o = dbl_group4(o);
+      if (active && (t & 3) == 0)
+        part[target] = curve::add(part[target], o);
     }
     __syncthreads();
   }
   if (t == 0) {
     fe x, y;
-    const bool infinity = curve::to_affine_standard(q, x, y);
+    const bool infinity = curve::to_affine_standard(part[0], x, y);
     for (int i = 0; i < 8; i++) {
       point->x[i] = x.l[i];
       point->y[i] = y.l[i];
