@@ -101,18 +101,23 @@ plan make_plan(unsigned n, unsigned window_bits, int sms) {
 // Host-resident inputs are processed in chunks of points: the copy of chunk
 // j + 1 runs on a helper stream while chunk j is sorted and accumulated, and
 // every chunk after the first accumulates into its own buckets, which are then
-// folded into the MSM's.  Chunk sizes grow by CHUNK_GROWTH (the pipeline takes
-// about five times as long per point as the host-to-device copy), so only the
-// first chunk's copy is exposed; the chunk count trades that copy against
-// one bucket fold and one more pipeline start per extra chunk (cost model
-// below, in microseconds, fitted to B200 measurements: at 2^22 two chunks
-// beat three, 12.72 vs 12.90 ms end to end).  Reference counterpart: the
+// folded into the MSM's.  Chunk sizes grow by CHUNK_GROWTH (a chunk's pipeline
+// takes about five times as long per point as the host-to-device copy, so
+// chunk j + 1's copy ends about when chunk j's work does), and only the first
+// chunk's copy is exposed; the chunk count trades that copy against one bucket
+// fold and one more pipeline start per extra chunk (cost model below, in
+// microseconds, fitted to B200 measurements).  Measured at 2^22 end to end:
+// two chunks 1:5 12.94 ms, 1:6 13.11 ms (chunk 1's copy outlasts chunk 0's
+// work), 1:4 level with 1:5, 1:3 slower; three chunks 1:4:16 13.13 ms.
+// Folding by continuing the earlier chunks' buckets inside the accumulation
+// (no second bucket set, no fold kernel) measured slower: 13.02 against
+// 12.85 ms at 2^22, 25.2 against 23.4 ms at 2^23.  Reference counterpart: the
 // chunked copy/compute overlap of schedule_execution (src/msm.cu:160-334).
 #ifndef MSM_MAX_CHUNKS
 #define MSM_MAX_CHUNKS 4
 #endif
 #ifndef MSM_CHUNK_GROWTH
-#define MSM_CHUNK_GROWTH 6
+#define MSM_CHUNK_GROWTH 5
 #endif
 constexpr unsigned MAX_CHUNKS = MSM_MAX_CHUNKS;
 constexpr unsigned CHUNK_GROWTH = MSM_CHUNK_GROWTH;
