@@ -67,8 +67,11 @@ static device_info get_device_info(int device) {
 // Accumulation ranges: a whole number k <= per_thread of ranges per thread,
 // as large as keeps ACC_MIN_RANGE entries per range (a range's start-up --
 // cursor search, first gather, head -- costs about as much as a few hundred
-// additions: 2^21 points ran 3 % slower with 256-entry ranges).  Whole
-// multiples keep every warp at the same number of rounds.
+// additions: 2^21 points ran 3 % slower with 205-entry ranges than with 410).
+// Whole multiples keep every warp at the same number of rounds.  Measured at
+// the 3.5M-point second chunk of a host-input 2^22 MSM (52 M entries): two
+// ranges of 346 entries per thread beat one of 692 by 0.48 ms (end to end
+// 12.90 -> 12.40 ms), hence 300 rather than 400.
 unsigned accumulation_ranges(unsigned threads, unsigned long long entries, unsigned per_thread) {
   const unsigned long long fit = entries / ((unsigned long long)threads * ACC_MIN_RANGE);
   const unsigned long long k = std::max(1ull, std::min((unsigned long long)per_thread, fit));

@@ -45,7 +45,7 @@ constexpr unsigned PROFILE_STAGES = 6;
 #define BATCH_ACC_RANGES_PER_THREAD 1
 #endif
 #ifndef ACC_MIN_RANGE
-#define ACC_MIN_RANGE 400 // entries a range keeps at least when ranges are multiplied
+#define ACC_MIN_RANGE 300 // entries a range keeps at least when ranges are multiplied
 #endif
 
 // Per-window sums of the reduction (reduce_groups_kernel, then one
