@@ -187,7 +187,7 @@ static layout make_layout(const plan &p, bool copy_scalars, bool copy_bases, boo
   };
   if (!copy_n)
     copy_n = p.n;
-  const size_t entries = (size_t)p.windows * p.n;
+  const size_t entries = (size_t)p.windows * window_stride(p.n);
   for (int i = 0; i < 2; i++) {
     l.keys[i] = take(entries * 4);
     l.vals[i] = take(entries * 4);
@@ -612,7 +612,7 @@ template <class F> static cudaError_t set_carveout(F *func, int percent) {
 cudaError_t set_up() {
   CHECK(cudaFuncSetAttribute(digits_histogram_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              MAX_FUSED_HISTOGRAM_WINDOWS * (SORT_RADIX + 1) * 4));
-  CHECK(set_carveout(accumulate_kernel, ACC_CARVEOUT)); // 4 blocks x 18 KB of base-point slots
+  CHECK(set_carveout(accumulate_kernel, ACC_CARVEOUT)); // 4 blocks x 19 KB of base-point slots and window bounds
   CHECK(set_carveout(merge_heads_kernel, cudaSharedmemCarveoutMaxL1));
   CHECK(set_carveout(reduce_groups_kernel, cudaSharedmemCarveoutMaxL1));
   CHECK(set_carveout(reduce_level_kernel, cudaSharedmemCarveoutMaxL1));

@@ -10,7 +10,7 @@ __global__ void __launch_bounds__(256) digits_kernel(const fe *__restrict__ scal
   if (i >= n)
     return;
   scalar_digits(load_fe_streaming(scalars + i), c, windows, [&](unsigned w, uint32_t magnitude, uint32_t negative) {
-    const size_t out = (size_t)w * n + i;
+    const size_t out = w * window_stride(n) + i;
     keys[out] = digit_key(magnitude);
     vals[out] = i | (negative << 31);
   });
@@ -29,13 +29,14 @@ __global__ void __launch_bounds__(SORT_THREADS) digits_histogram_kernel(const fe
   for (unsigned k = threadIdx.x; k < windows * (SORT_RADIX + 1); k += blockDim.x)
     hist[k] = 0;
   __syncthreads();
+  const size_t stride = window_stride(n);
   auto tile_digits = [&](auto width) {
     constexpr unsigned C = decltype(width)::value;
     for (unsigned k = 0; k < SORT_ITEMS; k++) {
       const unsigned i = tile * SORT_TILE + k * SORT_THREADS + threadIdx.x;
       if (i < n)
         scalar_digits_fixed<C>(load_fe_streaming(scalars + i), c, windows, [&](unsigned w, uint32_t magnitude, uint32_t negative) {
-          const size_t out = (size_t)w * n + i;
+          const size_t out = w * stride + i;
           const uint32_t key = digit_key(magnitude);
           keys[out] = key;
           vals[out] = i | (negative << 31);
@@ -67,8 +68,8 @@ __global__ void __launch_bounds__(SORT_THREADS) digits_histogram_kernel(const fe
 //    position is digit_base + counts + its rank among equal digits in the tile.
 //    The first pass drops zero digits (they add nothing to any bucket): it
 //    counts them into zeros[w] and writes the nonzero entries of window w to
-//    [w n + zeros[w], (w + 1) n); later passes sort that range only (tiles
-//    past its end have nothing to do).
+//    [w S + zeros[w], w S + n), S = window_stride(n); later passes sort that
+//    range only (tiles past its end have nothing to do).
 // ---------------------------------------------------------------------------
 template <bool FIRST>
 __device__ __forceinline__ void sort_histogram_window(const uint32_t *__restrict__ keys, unsigned n, unsigned tiles, unsigned shift,
@@ -76,7 +77,7 @@ __device__ __forceinline__ void sort_histogram_window(const uint32_t *__restrict
   const unsigned tile = blockIdx.x, w = blockIdx.y;
   const unsigned skip = FIRST ? 0 : zeros[w], live = n - skip;
   const unsigned base = tile * SORT_TILE;
-  sort_histogram_tile<FIRST>(keys + (size_t)w * n + skip, base, base < live ? min(SORT_TILE, live - base) : 0, shift,
+  sort_histogram_tile<FIRST>(keys + w * window_stride(n) + skip, base, base < live ? min(SORT_TILE, live - base) : 0, shift,
                              counts + (size_t)w * SORT_RADIX * tiles + tile, tiles, zeros + w);
 }
 
@@ -106,7 +107,7 @@ __global__ void __launch_bounds__(SORT_THREADS, 3) sort_scatter_first_kernel(con
                                                                           const uint32_t *__restrict__ zeros) {
   const unsigned tile = blockIdx.x, w = blockIdx.y;
   const unsigned base = tile * SORT_TILE;
-  const size_t seg = (size_t)w * n;
+  const size_t seg = w * window_stride(n);
   sort_scatter_tile<false, true>(keys_in, vals_in, keys_out, vals_out, seg, seg + zeros[w], base, min(SORT_TILE, n - base), shift,
                                  counts + (size_t)w * SORT_RADIX * tiles + tile, tiles, totals + (size_t)w * SORT_RADIX);
 }
@@ -121,7 +122,7 @@ __global__ void __launch_bounds__(SORT_THREADS, 3) sort_scatter_stable_kernel(co
   const unsigned base = tile * SORT_TILE;
   if (base >= live)
     return;
-  const size_t seg = (size_t)w * n + skip;
+  const size_t seg = w * window_stride(n) + skip;
   sort_scatter_tile<true, false>(keys_in, vals_in, keys_out, vals_out, seg, seg, base, min(SORT_TILE, live - base), shift,
                                  counts + (size_t)w * SORT_RADIX * tiles + tile, tiles, totals + (size_t)w * SORT_RADIX);
 }
@@ -131,18 +132,18 @@ __global__ void __launch_bounds__(SORT_THREADS, 3) sort_scatter_stable_kernel(co
 // ---------------------------------------------------------------------------
 constexpr unsigned MAX_WINDOWS = 128;
 
-// The plain pipeline's segments: window w holds entries [w n, (w + 1) n), its
-// nonzero entries last; bucket slot of a key = (w << log_b) | key_slot(key).
+// The plain pipeline's segments: window w holds entries [w S, w S + n)
+// (S = window_stride(n)), its nonzero entries last; bucket slot of a key = (w << log_b) | key_slot(key).
 struct window_segments {
   const affine *__restrict__ bases;
-  const uint32_t *s_zeros;            // shared: zero-digit prefix per window
+  const unsigned long long *s_first;  // shared: first nonzero entry of window w, then one past its last
   const unsigned long long *s_prefix; // shared: nonzero entries before window w
-  unsigned n, windows, log_b;
+  unsigned windows, log_b;
   __device__ __forceinline__ unsigned count() const { return windows; }
   __device__ __forceinline__ unsigned long long prefix(unsigned w) const { return s_prefix[w]; }
-  __device__ __forceinline__ size_t first(unsigned w) const { return (size_t)w * n + s_zeros[w]; }
-  __device__ __forceinline__ size_t end(unsigned w) const { return (size_t)(w + 1) * n; }
-  __device__ __forceinline__ bool empty(unsigned w) const { return s_zeros[w] == n; }
+  __device__ __forceinline__ size_t first(unsigned w) const { return s_first[2 * w]; }
+  __device__ __forceinline__ size_t end(unsigned w) const { return s_first[2 * w + 1]; }
+  __device__ __forceinline__ bool empty(unsigned w) const { return s_first[2 * w] == s_first[2 * w + 1]; }
   __device__ __forceinline__ unsigned bucket(unsigned w, uint32_t key) const { return (w << log_b) | key_slot(key, (1u << log_b) - 1); }
   __device__ __forceinline__ const affine *base(unsigned, uint32_t val) const { return bases + (val & 0x7fffffffu); }
 };
@@ -152,22 +153,25 @@ __global__ void __launch_bounds__(ACC_THREADS, ACC_MIN_BLOCKS) accumulate_kernel
                                                                  const uint32_t *__restrict__ zeros, unsigned ranges, unsigned *__restrict__ work,
                                                                  xyzz *__restrict__ buckets, uint8_t *__restrict__ flags,
                                                                  uint32_t *__restrict__ head_bucket, xyzz *__restrict__ head_point) {
-  __shared__ uint32_t s_zeros[MAX_WINDOWS];
+  __shared__ unsigned long long s_first[2 * MAX_WINDOWS];
   __shared__ unsigned long long s_prefix[MAX_WINDOWS + 1];
   __shared__ uint4 s_base[2][4][ACC_THREADS];
-  for (unsigned w = threadIdx.x; w < windows; w += blockDim.x)
-    s_zeros[w] = zeros[w];
+  const size_t stride = window_stride(n);
+  for (unsigned w = threadIdx.x; w < windows; w += blockDim.x) {
+    s_first[2 * w] = w * stride + zeros[w];
+    s_first[2 * w + 1] = w * stride + n;
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
     unsigned long long acc = 0;
     for (unsigned w = 0; w < windows; w++) {
       s_prefix[w] = acc;
-      acc += n - s_zeros[w];
+      acc += s_first[2 * w + 1] - s_first[2 * w];
     }
     s_prefix[windows] = acc;
   }
   __syncthreads();
-  const window_segments seg{bases, s_zeros, s_prefix, n, windows, log_b};
+  const window_segments seg{bases, s_first, s_prefix, windows, log_b};
   accumulate_ranges(seg, keys, vals, ranges, work, buckets, flags, head_bucket, head_point, s_base);
 }
 

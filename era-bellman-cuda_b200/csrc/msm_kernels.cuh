@@ -46,6 +46,12 @@ constexpr unsigned SORT_ITEMS = 16; // per thread; a tile is SORT_THREADS * SORT
 constexpr unsigned SORT_TILE = SORT_THREADS * SORT_ITEMS;
 constexpr unsigned ACC_THREADS = 128;
 
+// Window w's entries start at w * window_stride(n): n rounded up to 32
+// entries, so that every window segment starts on a 128-byte line and the
+// digit kernels' stores stay whole lines whatever n is (at n = 3,495,254
+// the digit stage took 0.220 ms, at the aligned 3,495,264 0.141 ms).
+__host__ __device__ __forceinline__ size_t window_stride(unsigned n) { return ((size_t)n + 31) & ~(size_t)31; }
+
 // Launch geometry of the whole pipeline, computed on the host.
 struct plan {
   unsigned n;           // points
