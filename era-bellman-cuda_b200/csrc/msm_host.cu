@@ -111,7 +111,9 @@ plan make_plan(unsigned n, unsigned window_bits, int sms) {
 // fold and one more pipeline start per extra chunk (cost model below, in
 // microseconds, fitted to B200 measurements).  Measured at 2^22 end to end:
 // two chunks 1:5 12.94 ms, 1:6 13.11 ms (chunk 1's copy outlasts chunk 0's
-// work), 1:4 level with 1:5, 1:3 slower; three chunks 1:4:16 13.13 ms.
+// work), 1:4 level with 1:5, 1:3 slower; three chunks 1:4:16 13.13 ms.  With
+// the later accumulation-range and segment-alignment fixes, three chunks 1:5:25
+// still lose to two: 12.30 against 12.27 ms.
 // Folding by continuing the earlier chunks' buckets inside the accumulation
 // (no second bucket set, no fold kernel) measured slower: 13.02 against
 // 12.85 ms at 2^22, 25.2 against 23.4 ms at 2^23.  Reference counterpart: the
@@ -125,7 +127,10 @@ plan make_plan(unsigned n, unsigned window_bits, int sms) {
 constexpr unsigned MAX_CHUNKS = MSM_MAX_CHUNKS;
 constexpr unsigned CHUNK_GROWTH = MSM_CHUNK_GROWTH;
 constexpr double COPY_US_PER_POINT = 0.58e-3; // 32 B scalar over PCIe
-constexpr double EXTRA_CHUNK_US = 360.0;      // one bucket fold + one more pipeline start
+#ifndef MSM_EXTRA_CHUNK_US
+#define MSM_EXTRA_CHUNK_US 360.0
+#endif
+constexpr double EXTRA_CHUNK_US = MSM_EXTRA_CHUNK_US; // one bucket fold + one more pipeline start
 constexpr unsigned MIN_FIRST_CHUNK = 1u << 16;
 
 struct chunking {
