@@ -9,7 +9,8 @@
 // A batch is a fixed list of instance sizes n_k (any lengths, prefixes of the
 // table).  All instances run as one kernel chain:
 //   digits       every point of every instance, W(c_k) signed digits each, into
-//                its instance's segment of W(c_k) * n_k (key, value) entries
+//                its instance's segment of W(c_k) windows of window_stride(n_k)
+//                (key, value) entries (the padding holds zero digits)
 //   sort         segmented LSD radix sort, tile list over all segments; the
 //                first pass drops zero digits (counted per segment)
 //   accumulate   the nonzero entries of all segments split into equal ranges,
@@ -115,13 +116,22 @@ __global__ void __launch_bounds__(256) batch_digits_kernel(const batch_instance 
   const batch_instance d = inst[k];
   const fe *scalars = io[k].scalars;
   const fe scalar = load_fe_streaming(scalars + i);
+  const size_t window_base = d.entry_offset, stride = window_stride(d.n);
   auto digits = [&](auto width) {
     scalar_digits_fixed<decltype(width)::value>(scalar, d.c, d.windows, [&](unsigned w, uint32_t magnitude, uint32_t negative) {
-      const size_t out = d.entry_offset + (size_t)w * d.n + i;
+      const size_t out = window_base + w * stride + i;
       keys[out] = digit_key(magnitude);
       vals[out] = (w * d.stride + i) | (negative << 31);
     });
   };
+  // the padding after each window (its segment is window_stride(n) long)
+  // holds zero digits, which the first sort pass drops; point i fills padding
+  // slots i, i + n, ... (an instance may have fewer points than padding slots)
+  for (size_t j = i; j < stride - d.n; j += d.n)
+    for (unsigned w = 0; w < d.windows; w++) {
+      keys[window_base + w * stride + d.n + j] = ZERO_KEY;
+      vals[window_base + w * stride + d.n + j] = 0;
+    }
   // the widths the batch table picks for its large instances get unrolled code
   switch (d.c) {
   case 16: digits(width_constant<16>{}); break;
@@ -440,9 +450,9 @@ cudaError_t make_batch_plan(batch_plan &b, const base_table_impl *table, const u
     d.windows = windows_for(c);
     d.stride = table->prefix[c];
     d.table = table->mult[c];
-    if ((unsigned long long)d.windows * n >= (1ull << 31) || d.windows * (unsigned long long)d.stride >= (1ull << 31))
+    if ((unsigned long long)d.windows * window_stride(n) >= (1ull << 31) || d.windows * (unsigned long long)d.stride >= (1ull << 31))
       return cudaErrorInvalidValue;
-    d.entries = d.windows * n;
+    d.entries = d.windows * (unsigned)window_stride(n); // windows start on 128-byte lines (window_stride)
     d.entry_offset = b.total_entries;
     d.tiles = (d.entries + SORT_TILE - 1) / SORT_TILE;
     d.tile_base = b.total_tiles;

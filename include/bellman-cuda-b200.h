@@ -128,7 +128,8 @@ bc_error msm_b200_batch_create(msm_b200_batch *batch, msm_b200_base_table table,
  * results[k] (254 Jacobian points) are device pointers.  Executions of one
  * batch share its scratch: serialise them (one stream). */
 bc_error msm_b200_batch_execute_async(msm_b200_batch batch, const void *const *scalars, void *const *results, bc_stream stream);
-/* Scratch bytes, kernels in the graph, and (window, point) entries of a batch. */
+/* Scratch bytes, kernels in the graph, and (window, point) entries of a batch
+ * (each window padded to a multiple of 32 points). */
 bc_error msm_b200_batch_info(msm_b200_batch batch, size_t *scratch_bytes, unsigned *kernels, unsigned long long *entries);
 bc_error msm_b200_batch_destroy(msm_b200_batch batch);
 
