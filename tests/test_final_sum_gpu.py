@@ -148,3 +148,49 @@ def test_invalid_arguments(gpu):
     bc.stream_synchronize(gpu.stream)
     bc.free(rd)
     bc.free(pd)
+
+
+def test_pinned_results_input(gpu, oracle):
+    """Results in pinned host memory (msm_execute_async writes them there when
+    the caller passes host results) are read in place through their device alias."""
+    import bellman_cuda as bcm
+    bc = gpu.bc
+    bases, scalars, k = H.table_workload(1 << 11, 41)
+    res = gpu.msm(bases, scalars)
+    view, ptr = bc.pinned_array((254, 24))
+    view[...] = res
+    pd = bc.malloc(ctypes.sizeof(bcm.AffinePoint))
+    assert bc.final_sum_async(ptr, pd, gpu.stream) == 0
+    bc.stream_synchronize(gpu.stream)
+    point = bcm.AffinePoint.from_buffer_copy(bc.from_device(pd, (20,)).tobytes()).as_tuple()
+    bc.free(pd)
+    bc.free_host(ptr)
+    assert point == oracle.msm_checksum(k, scalars)
+
+
+def test_batched_results(gpu, oracle):
+    """The 254 results of batched instances (one window's partial sums per bit
+    position, precomputed multiples) reduce to each instance's MSM."""
+    bc = gpu.bc
+    n = 5000
+    k = synth.base_multipliers(47, n)
+    kd = gpu.upload(k)
+    bd = bc.malloc(n * 64)
+    bc.generator_multiples(kd, bd, n, gpu.stream)
+    bc.stream_synchronize(gpu.stream)
+    table = bc.base_table_create(bd, n, gpu.stream)
+    bc.stream_synchronize(gpu.stream)
+    lengths = [n, 1, 777]
+    work = [synth.uniform_scalars(700 + j, m) for j, m in enumerate(lengths)]
+    batch = bc.batch_create(table, lengths)
+    sd = [gpu.upload(s) for s in work]
+    rd = [bc.malloc(254 * 96) for _ in lengths]
+    bc.batch_execute(batch, sd, rd, gpu.stream)
+    bc.stream_synchronize(gpu.stream)
+    for m, s, r in zip(lengths, work, rd):
+        res = bc.from_device(r, (254, 24))
+        assert final_sum(gpu, res) == oracle.msm_checksum(k[:m], s) == oracle.horner(res)
+    bc.batch_destroy(batch)
+    bc.base_table_destroy(table)
+    for p in sd + rd + [kd, bd]:
+        bc.free(p)
