@@ -91,8 +91,12 @@ __global__ void __launch_bounds__(FINAL_THREADS) final_sum_kernel(const jacobian
     if (((t & ~31u) >> 2) < pairs) { // warp-uniform: the warp's first group is active
       const bool active = group < pairs;
       xyzz o = part[active ? partner : 0];
-      for (unsigned k = 0; k < (1u << level); k++)
-        o = dbl_group4(o);
+      // the double of infinity is infinity: a warp whose active partners are
+      // all infinity skips the chain (the batched path's results are
+      // infinity above bit c - 1, so most of its chains are skipped)
+      if (!__all_sync(0xffffffffu, !active || curve::is_inf(o)))
+        for (unsigned k = 0; k < (1u << level); k++)
+          o = dbl_group4(o);
       if (active && (t & 3) == 0)
         part[target] = curve::add(part[target], o);
     }
