@@ -178,3 +178,39 @@ def test_model_matches_sum(trial):
         scal = [rng.choice([0, 0, 1, 1, rng.randrange(1 << 16), rng.randrange(R)]) for _ in range(n)]
     kl = [rng.randrange(1, R) for _ in range(n)]
     assert model_msm(scal, kl, c, T) == sum(s * k for s, k in zip(scal, kl)) % R
+
+
+def model_final_sum(values, threads=128, result_bits=254):
+    """The index arithmetic of final_sum_kernel (msm_final.cu) with points as
+    integers mod R (doubling = 2x, addition = x + y): level 0 per thread
+    (R_2t + 2 R_2t+1), level 1 per even thread (partner doubled twice),
+    levels 2..7 per group of four lanes, group g adding part[g 2^L + 2^(L-1)]
+    doubled 2^L times into part[g 2^L].  Every partner index must stay in
+    the block and be read before anyone writes it at that level."""
+    part = [0] * threads
+    for t in range(threads):
+        if 2 * t + 1 < result_bits:
+            part[t] = (values[2 * t] + 2 * values[2 * t + 1]) % R
+    for t in range(0, threads, 2):
+        part[t] = (part[t] + 4 * part[t + 1]) % R
+    level = 2
+    while (1 << level) <= threads:
+        pairs = threads >> level
+        targets, partners = set(), set()
+        for group in range(threads // 4):
+            if group < pairs:
+                target, partner = group << level, (group << level) + (1 << (level - 1))
+                assert partner < threads
+                targets.add(target)
+                partners.add(partner)
+                part[target] = (part[target] + pow(2, 1 << level, R) * part[partner]) % R
+        assert not targets & partners  # no group reads a slot another group writes
+        level += 1
+    return part[0]
+
+
+@pytest.mark.parametrize("trial", range(6))
+def test_final_sum_tree(trial):
+    rng = random.Random(2000 + trial)
+    values = [rng.randrange(R) if rng.random() < 0.8 else 0 for _ in range(254)]
+    assert model_final_sum(values) == sum(v * pow(2, i, R) for i, v in enumerate(values)) % R
