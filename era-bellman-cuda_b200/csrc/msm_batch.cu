@@ -169,7 +169,7 @@ __global__ void __launch_bounds__(256) batch_sort_scan_kernel(uint32_t *counts, 
 }
 
 template <bool STABLE>
-__global__ void __launch_bounds__(SORT_THREADS, 3) batch_sort_scatter_kernel(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
+__global__ void __launch_bounds__(SORT_THREADS, SORT_SCATTER_MIN_BLOCKS) batch_sort_scatter_kernel(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
                                                                           uint32_t *__restrict__ keys_out, uint32_t *__restrict__ vals_out,
                                                                           const batch_instance *__restrict__ inst,
                                                                           const unsigned *__restrict__ tile_seg, unsigned shift,

@@ -100,7 +100,7 @@ __global__ void __launch_bounds__(256) sort_scan_kernel(uint32_t *counts, unsign
   sort_scan_row(counts + (size_t)row * tiles, tiles, totals + row);
 }
 
-__global__ void __launch_bounds__(SORT_THREADS, 3) sort_scatter_first_kernel(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
+__global__ void __launch_bounds__(SORT_THREADS, SORT_SCATTER_MIN_BLOCKS) sort_scatter_first_kernel(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
                                                                           uint32_t *__restrict__ keys_out, uint32_t *__restrict__ vals_out,
                                                                           unsigned n, unsigned tiles, unsigned shift,
                                                                           const uint32_t *__restrict__ counts, const uint32_t *__restrict__ totals,
@@ -112,7 +112,7 @@ __global__ void __launch_bounds__(SORT_THREADS, 3) sort_scatter_first_kernel(con
                                  counts + (size_t)w * SORT_RADIX * tiles + tile, tiles, totals + (size_t)w * SORT_RADIX);
 }
 
-__global__ void __launch_bounds__(SORT_THREADS, 3) sort_scatter_stable_kernel(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
+__global__ void __launch_bounds__(SORT_THREADS, SORT_SCATTER_MIN_BLOCKS) sort_scatter_stable_kernel(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
                                                                            uint32_t *__restrict__ keys_out, uint32_t *__restrict__ vals_out,
                                                                            unsigned n, unsigned tiles, unsigned shift,
                                                                            const uint32_t *__restrict__ counts, const uint32_t *__restrict__ totals,

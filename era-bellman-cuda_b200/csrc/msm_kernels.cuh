@@ -44,6 +44,11 @@ constexpr unsigned SORT_RADIX = 1u << SORT_RADIX_BITS;
 constexpr unsigned SORT_THREADS = 256;
 constexpr unsigned SORT_ITEMS = 16; // per thread; a tile is SORT_THREADS * SORT_ITEMS keys
 constexpr unsigned SORT_TILE = SORT_THREADS * SORT_ITEMS;
+// Resident scatter blocks per SM (4 caps registers at 64, with a few bytes of
+// spills): at 2^22 the sort stage took 1.067 ms at 3 blocks, 1.012 at 4.
+#ifndef SORT_SCATTER_MIN_BLOCKS
+#define SORT_SCATTER_MIN_BLOCKS 4
+#endif
 constexpr unsigned ACC_THREADS = 128;
 
 // Window w's entries start at w * window_stride(n): n rounded up to 32
