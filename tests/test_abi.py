@@ -115,3 +115,29 @@ def test_affine_point_layout_matches_ctypes(tmp_path):
     got = [int(v) for v in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
     A = bc.AffinePoint
     assert got == [ctypes.sizeof(A), A.y.offset, A.infinity.offset, A.reserved.offset] == [80, 32, 64, 68]
+
+
+def test_argument_checks_without_a_gpu(product_lib_path):
+    """The checks that come before any CUDA call (null, misaligned or
+    out-of-range arguments) return bc_error_invalid_value on a machine
+    without a GPU too; the size queries answer from the tuning tables."""
+    import bellman_cuda as bc
+    lib = bc.BellmanCuda(product_lib_path).lib
+    null_stream = bc.Handle()
+    invalid = bc.BC_ERROR_INVALID_VALUE
+    assert lib.msm_b200_final_sum_async(None, None, null_stream) == invalid
+    assert lib.msm_b200_final_sum_async(0x1008, 0x2000, null_stream) == invalid  # results not 16-byte aligned
+    assert lib.msm_b200_final_sum_async(0x1000, 0x2002, null_stream) == invalid  # point not 4-byte aligned
+    assert lib.msm_b200_execute_no_alloc_async(null_stream, None, 0x1000, 0x2000, 16) == invalid
+    assert lib.msm_b200_execute_no_alloc_async(null_stream, 0x1000, 0x2000, 0x3000, 0) == invalid
+    assert lib.msm_b200_execute_no_alloc_async(null_stream, 0x1000, 0x2000, 0x3000, bc.NO_ALLOC_MAX_COUNT + 1) == invalid
+    assert lib.msm_b200_execute_no_alloc_async(null_stream, 0x1008, 0x2000, 0x3000, 16) == invalid
+    assert lib.msm_b200_execute_async(None) == invalid
+    cfg = bc.MsmConfiguration()
+    cfg.log_scalars_count = 32
+    assert lib.msm_execute_async(cfg) == invalid
+    assert lib.msm_b200_batch_create(None, None, None, 0, None) == invalid
+    c = ctypes.c_uint()
+    assert lib.msm_b200_default_window_bits(0, ctypes.byref(c)) == invalid
+    assert lib.msm_b200_default_window_bits(1 << 22, ctypes.byref(c)) == 0 and c.value == 17
+    assert lib.msm_b200_batch_window_bits(1 << 22, ctypes.byref(c)) == 0 and c.value == 20
