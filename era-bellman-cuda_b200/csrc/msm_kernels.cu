@@ -243,7 +243,7 @@ __global__ void __launch_bounds__(ACC_THREADS) merge_chunk_buckets_kernel(xyzz *
 // holds |d| = B and is excluded here).  For i = m-1 .. 1: run += X, acc += run,
 // giving acc = sum_i i * X_{gm+i} and run = sum_i X_{gm+i}; then
 // S_w = sum_g acc_g + m * sum_g g * run_g.
-__global__ void __launch_bounds__(ACC_THREADS) reduce_groups_kernel(const xyzz *__restrict__ buckets, const uint8_t *__restrict__ flags,
+__global__ void __launch_bounds__(ACC_THREADS, REDUCE_GROUPS_MIN_BLOCKS) reduce_groups_kernel(const xyzz *__restrict__ buckets, const uint8_t *__restrict__ flags,
                                                                     unsigned windows, unsigned log_b, unsigned log_m, xyzz *__restrict__ run_out,
                                                                     xyzz *__restrict__ streams) {
   const unsigned log_g = log_b - log_m;
@@ -273,7 +273,7 @@ __global__ void __launch_bounds__(ACC_THREADS) reduce_groups_kernel(const xyzz *
 //   * every older stream takes one pairwise step, G >> level -> G >> (level+1).
 // All streams therefore shrink together and hold one sum each after the last
 // level.  Streams and tree are ping-ponged between levels (in = level & 1).
-__global__ void __launch_bounds__(ACC_THREADS) reduce_level_kernel(const xyzz *__restrict__ t_in, xyzz *__restrict__ t_out,
+__global__ void __launch_bounds__(ACC_THREADS, REDUCE_LEVEL_MIN_BLOCKS) reduce_level_kernel(const xyzz *__restrict__ t_in, xyzz *__restrict__ t_out,
                                                                    const xyzz *__restrict__ s_in, xyzz *__restrict__ s_out, unsigned windows,
                                                                    unsigned log_g, unsigned level) {
   const unsigned half = (1u << log_g) >> (level + 1);
