@@ -32,10 +32,19 @@ __global__ void __launch_bounds__(SORT_THREADS) digits_histogram_kernel(const fe
   const size_t stride = window_stride(n);
   auto tile_digits = [&](auto width) {
     constexpr unsigned C = decltype(width)::value;
+    // the next scalar is loaded before this one is decomposed, so that its
+    // load overlaps the decomposition, the stores and the counting
+    const unsigned first = tile * SORT_TILE + threadIdx.x;
+    fe next = fr::zero();
+    if (first < n)
+      next = load_fe_streaming(scalars + first);
     for (unsigned k = 0; k < SORT_ITEMS; k++) {
-      const unsigned i = tile * SORT_TILE + k * SORT_THREADS + threadIdx.x;
+      const unsigned i = first + k * SORT_THREADS;
+      const fe scalar = next;
+      if (k + 1 < SORT_ITEMS && i + SORT_THREADS < n)
+        next = load_fe_streaming(scalars + i + SORT_THREADS);
       if (i < n)
-        scalar_digits_fixed<C>(load_fe_streaming(scalars + i), c, windows, [&](unsigned w, uint32_t magnitude, uint32_t negative) {
+        scalar_digits_fixed<C>(scalar, c, windows, [&](unsigned w, uint32_t magnitude, uint32_t negative) {
           const size_t out = w * stride + i;
           const uint32_t key = digit_key(magnitude);
           keys[out] = key;
