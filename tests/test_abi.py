@@ -141,3 +141,37 @@ def test_argument_checks_without_a_gpu(product_lib_path):
     assert lib.msm_b200_default_window_bits(0, ctypes.byref(c)) == invalid
     assert lib.msm_b200_default_window_bits(1 << 22, ctypes.byref(c)) == 0 and c.value == 17
     assert lib.msm_b200_batch_window_bits(1 << 22, ctypes.byref(c)) == 0 and c.value == 20
+
+
+LINK_PROGRAM = r"""
+#include <stdio.h>
+#include "bellman-cuda.h"
+#include "bellman-cuda-b200.h"
+/* A C caller of the drop-in: the reference's msm_configuration by value, and
+   the extensions; run with no GPU it only exercises the argument checks. */
+int main(void) {
+  msm_configuration cfg = {0};
+  cfg.log_scalars_count = 40;
+  bc_stream stream = {0};
+  int a = msm_execute_async(cfg);
+  int b = msm_b200_final_sum_async(NULL, NULL, stream);
+  int c = msm_b200_execute_no_alloc_async(stream, NULL, NULL, NULL, 0);
+  unsigned bits = 0;
+  int d = msm_b200_default_window_bits(1u << 20, &bits);
+  printf("%d %d %d %d %u\n", a, b, c, d, bits);
+  return 0;
+}
+"""
+
+
+def test_c_caller_links_and_runs_without_a_gpu(product_lib_path, tmp_path):
+    """A C program includes both headers, links the shared library by name
+    (-lbellman_cuda_b200) and runs its argument checks on a machine without a GPU."""
+    src = tmp_path / "caller.c"
+    exe = tmp_path / "caller"
+    src.write_text(LINK_PROGRAM)
+    libdir = os.path.dirname(product_lib_path)
+    subprocess.run(["gcc", "-std=c11", "-I", INCLUDE, str(src), "-L", libdir, "-lbellman_cuda_b200", "-Wl,-rpath," + libdir, "-o", str(exe)],
+                   check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()
+    assert out == ["1", "1", "1", "0", "15"]
