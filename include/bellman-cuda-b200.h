@@ -212,11 +212,12 @@ bc_error msm_b200_execute_no_alloc_async(bc_stream stream, const void *bases, co
  * at infinity.  The bytes therefore compare equal for equal points, whatever
  * window split produced the R_i.
  *
- * `results` (16-byte aligned) and `point` must be device memory or pinned
- * host memory (registered or cudaMallocHost'd; the kernel reads and writes it
- * in place); a null or pageable pointer returns bc_error_invalid_value before
- * anything is enqueued.  Asynchronous on `stream`, one kernel of one block,
- * no allocation.  Enqueue it after the MSM on the same stream. */
+ * `results` (16-byte aligned) and `point` must be device memory of the
+ * current device (or memory it can reach) or pinned host memory (registered
+ * or cudaMallocHost'd; the kernel reads and writes it in place); a null or
+ * pageable pointer returns bc_error_invalid_value before anything is
+ * enqueued.  Asynchronous on `stream`, one kernel of one block, no
+ * allocation.  Enqueue it after the MSM on the same stream. */
 typedef struct msm_b200_affine_point {
   uint32_t x[8];
   uint32_t y[8];
