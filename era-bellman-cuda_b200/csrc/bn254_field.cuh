@@ -26,11 +26,7 @@
 // rarely taken paths (point doubling inside an addition) stay out of line so
 // the hot loop's instructions fit the instruction cache
 #define BN_HD_COLD __host__ __device__ __noinline__
-#if defined(BN254_OUTLINE_MUL)
-#define BN_HD_MUL __host__ __device__ __noinline__
-#else
 #define BN_HD_MUL __host__ __device__ __forceinline__
-#endif
 #else
 #define BN_HD inline
 #define BN_DEV inline
@@ -472,18 +468,7 @@ template <class F> struct field {
     return r;
   }
 
-#if defined(BN254_KARATSUBA)
-  // Montgomery product as a 512-bit Karatsuba product and one REDC (120
-  // multiply-unit instructions instead of CIOS's 136, see mul_wide_karatsuba).
-  // a, b < 2m give a*b < 4m^2, so redc_wide returns a value < 2m.
-  // Measured on a B200 (accumulation at 2^22): 11.41 ms against CIOS's 9.81 ms,
-  // and Karatsuba in mul_sub_mul only (BN254_KARATSUBA_WIDE) 9.95 ms: the
-  // extra carry-chain additions lengthen the dependent chains more than the
-  // saved multiplies shorten the busy multiply pipe, so CIOS stays the default.
-  static BN_HD_MUL fe mul(const fe &a, const fe &b) { return redc_wide(mul_wide_karatsuba(a, b)); }
-#else
   static BN_HD_MUL fe mul(const fe &a, const fe &b) { return mul_cios(a, b); }
-#endif
 
   static BN_HD_MUL fe mul_cios(const fe &a, const fe &b) {
     uint32_t X[17], Y[17];
@@ -576,125 +561,6 @@ template <class F> struct field {
     for (int k = 1; k < 15; k++)
       w.l[k] = cc::addc_cc(E[k], O[k]);
     w.l[15] = cc::addc(E[15], O[15]);
-    return w;
-  }
-
-  // --- 4-limb building blocks of the Karatsuba product -----------------------
-  // A[R..R+3] += x[0,2] * y (word pairs (R, R+1), (R+2, R+3)); carry into A[R+4]
-  template <int R> static BN_HD void even_products4(uint32_t *A, const uint32_t *x, uint32_t y) {
-    A[R + 0] = cc::mad_lo_cc(x[0], y, A[R + 0]);
-    A[R + 1] = cc::madc_hi_cc(x[0], y, A[R + 1]);
-    A[R + 2] = cc::madc_lo_cc(x[2], y, A[R + 2]);
-    A[R + 3] = cc::madc_hi_cc(x[2], y, A[R + 3]);
-    A[R + 4] = cc::addc(A[R + 4], 0);
-  }
-  // B[R+1..R+4] += x[1,3] * y, no carry out
-  template <int R> static BN_HD void odd_products4(uint32_t *B, const uint32_t *x, uint32_t y) {
-    B[R + 1] = cc::mad_lo_cc(x[1], y, B[R + 1]);
-    B[R + 2] = cc::madc_hi_cc(x[1], y, B[R + 2]);
-    B[R + 3] = cc::madc_lo_cc(x[3], y, B[R + 3]);
-    B[R + 4] = cc::madc_hi(x[3], y, B[R + 4]);
-  }
-  template <int I> static BN_HD void wide_row4(uint32_t *E, uint32_t *O, const uint32_t *x, uint32_t y) {
-    if (I % 2 == 0) {
-      even_products4<I>(E, x, y);
-      odd_products4<I>(O, x, y);
-    } else {
-      even_products4<I>(O, x, y);
-      odd_products4<I>(E, x, y);
-    }
-  }
-
-  // 128 x 128 -> 256-bit product of 4-limb operands (32 multiply instructions),
-  // with the even/odd word-pair accumulators of mul_wide (row i's partial sum
-  // is < 2^(32(i+5)), so the chain ending at word i+3 carries into a fresh
-  // word i+4 and the one ending at word i+4 never carries out).
-  static BN_HD void mul4_wide(const uint32_t *x, const uint32_t *y, uint32_t *out) {
-    uint32_t E[9], O[9];
-#pragma unroll
-    for (int k = 0; k < 9; k++) {
-      E[k] = 0;
-      O[k] = 0;
-    }
-    E[0] = cc::mul_lo(x[0], y[0]);
-    E[1] = cc::mul_hi(x[0], y[0]);
-    E[2] = cc::mul_lo(x[2], y[0]);
-    E[3] = cc::mul_hi(x[2], y[0]);
-    O[1] = cc::mul_lo(x[1], y[0]);
-    O[2] = cc::mul_hi(x[1], y[0]);
-    O[3] = cc::mul_lo(x[3], y[0]);
-    O[4] = cc::mul_hi(x[3], y[0]);
-    wide_row4<1>(E, O, x, y[1]);
-    wide_row4<2>(E, O, x, y[2]);
-    wide_row4<3>(E, O, x, y[3]);
-    out[0] = cc::add_cc(E[0], O[0]);
-#pragma unroll
-    for (int k = 1; k < 7; k++)
-      out[k] = cc::addc_cc(E[k], O[k]);
-    out[7] = cc::addc(E[7], O[7]);
-  }
-
-  // |u - v| of 4-limb values; returns the sign mask (0xffffffff when u < v)
-  static BN_HD uint32_t abs_diff4(const uint32_t *u, const uint32_t *v, uint32_t *d) {
-    d[0] = cc::sub_cc(u[0], v[0]);
-    d[1] = cc::subc_cc(u[1], v[1]);
-    d[2] = cc::subc_cc(u[2], v[2]);
-    d[3] = cc::subc_cc(u[3], v[3]);
-    const uint32_t m = cc::subc(0, 0);
-    // (d ^ m) - m: two's complement negation when m is all ones
-    d[0] = cc::sub_cc(d[0] ^ m, m);
-    d[1] = cc::subc_cc(d[1] ^ m, m);
-    d[2] = cc::subc_cc(d[2] ^ m, m);
-    d[3] = cc::subc(d[3] ^ m, m);
-    return m;
-  }
-
-  // Full 512-bit product by one level of subtractive Karatsuba over 128-bit
-  // halves a = a0 + a1 2^128, b = b0 + b1 2^128:
-  //   z0 = a0 b0, z2 = a1 b1, zm = |a0 - a1| |b0 - b1|,
-  //   a0 b1 + a1 b0 = z0 + z2 - (a0 - a1)(b0 - b1) = z0 + z2 -/+ zm
-  // (minus when the two differences have the same sign).  96 multiply
-  // instructions instead of 128; the middle term z1 < 2^257 takes nine words.
-  static BN_HD fe_wide mul_wide_karatsuba(const fe &a, const fe &b) {
-    uint32_t z0[8], z2[8], zm[8], da[4], db[4];
-    mul4_wide(a.l, b.l, z0);
-    mul4_wide(a.l + 4, b.l + 4, z2);
-    const uint32_t sa = abs_diff4(a.l, a.l + 4, da);
-    const uint32_t sb = abs_diff4(b.l, b.l + 4, db);
-    mul4_wide(da, db, zm);
-    // t = z0 + z2 (nine words)
-    uint32_t t[9];
-    t[0] = cc::add_cc(z0[0], z2[0]);
-#pragma unroll
-    for (int k = 1; k < 8; k++)
-      t[k] = cc::addc_cc(z0[k], z2[k]);
-    t[8] = cc::addc(0, 0);
-    // z1 = t + (zm ^ n) + (n & 1) with n = all ones when zm is subtracted
-    // (the nine-word two's complement of zm), n = 0 when it is added
-    const uint32_t n = ~(sa ^ sb);
-    uint32_t z1[9];
-    (void)cc::add_cc(n, n); // carry flag = n & 1
-#pragma unroll
-    for (int k = 0; k < 8; k++)
-      z1[k] = cc::addc_cc(t[k], zm[k] ^ n);
-    z1[8] = cc::addc(t[8], n);
-    // w = z0 + z1 2^128 + z2 2^256
-    fe_wide w;
-#pragma unroll
-    for (int k = 0; k < 4; k++)
-      w.l[k] = z0[k];
-    w.l[4] = cc::add_cc(z0[4], z1[0]);
-    w.l[5] = cc::addc_cc(z0[5], z1[1]);
-    w.l[6] = cc::addc_cc(z0[6], z1[2]);
-    w.l[7] = cc::addc_cc(z0[7], z1[3]);
-    w.l[8] = cc::addc_cc(z2[0], z1[4]);
-    w.l[9] = cc::addc_cc(z2[1], z1[5]);
-    w.l[10] = cc::addc_cc(z2[2], z1[6]);
-    w.l[11] = cc::addc_cc(z2[3], z1[7]);
-    w.l[12] = cc::addc_cc(z2[4], z1[8]);
-    w.l[13] = cc::addc_cc(z2[5], 0);
-    w.l[14] = cc::addc_cc(z2[6], 0);
-    w.l[15] = cc::addc(z2[7], 0);
     return w;
   }
 
@@ -793,22 +659,13 @@ template <class F> struct field {
     return out;
   }
 
-#if defined(BN254_SQR_AS_MUL)
-  static BN_HD_MUL fe sqr(const fe &a) { return mul(a, a); }
-#else
   static BN_HD_MUL fe sqr(const fe &a) { return redc_wide(sqr_wide(a)); }
-#endif
 
   // a*b - c*d with one reduction: both products < 4m^2; a negative
   // difference is lifted by 4m^2, so the reduced operand is in [0, 4m^2).
   static BN_HD_MUL fe mul_sub_mul(const fe &a, const fe &b, const fe &c, const fe &d) {
-#if defined(BN254_KARATSUBA) || defined(BN254_KARATSUBA_WIDE)
-    fe_wide x = mul_wide_karatsuba(a, b);
-    const fe_wide y = mul_wide_karatsuba(c, d);
-#else
     fe_wide x = mul_wide(a, b);
     const fe_wide y = mul_wide(c, d);
-#endif
     x.l[0] = cc::sub_cc(x.l[0], y.l[0]);
 #pragma unroll
     for (int i = 1; i < 16; i++)

@@ -34,8 +34,8 @@ __global__ void __launch_bounds__(256) mad_peak_kernel(uint32_t seed, unsigned i
   sink[tid] = x;
 }
 
-// kinds 4 / 5: sixteen independent mad.lo (4) or mad.hi (5) per iteration
-template <bool HI> __global__ void __launch_bounds__(256) mad_half_kernel(uint32_t seed, unsigned iters, uint32_t *sink) {
+// kind 4: sixteen independent mad.lo per iteration
+__global__ void __launch_bounds__(256) mad_lo_kernel(uint32_t seed, unsigned iters, uint32_t *sink) {
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
   uint32_t acc[16];
   const uint32_t b = seed ^ (tid * 0x9e3779b9u), c = seed + tid;
@@ -45,10 +45,7 @@ template <bool HI> __global__ void __launch_bounds__(256) mad_half_kernel(uint32
   for (unsigned i = 0; i < iters; i++) {
 #pragma unroll
     for (int j = 0; j < 16; j++) {
-      if (HI)
-        asm volatile("mad.hi.u32 %0, %0, %1, %2;" : "+r"(acc[j]) : "r"(b), "r"(c));
-      else
-        asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(acc[j]) : "r"(b), "r"(c));
+      asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(acc[j]) : "r"(b), "r"(c));
     }
   }
   uint32_t x = 0;
@@ -113,86 +110,6 @@ __global__ void __launch_bounds__(128) montmul_kernel(uint32_t seed, unsigned it
   sink[tid] = x.l[0] ^ z.l[1];
 }
 
-// kinds 6..9: component throughput (two independent chains per thread)
-//   6: squaring (208 multiply instructions), 7: a*b - c*d (392),
-//   8: 512-bit product (128), 9: field add + sub pairs (no multiplies; counted as 2 per pair)
-template <int KIND> __global__ void __launch_bounds__(128) component_kernel(uint32_t seed, unsigned iters, uint32_t *sink) {
-  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
-  fe x, y, z, w;
-#pragma unroll
-  for (int j = 0; j < 8; j++) {
-    x.l[j] = (seed * (j + 7)) ^ tid;
-    y.l[j] = (seed + j) * 0x2545f491u;
-    z.l[j] = tid * (j + 1);
-    w.l[j] = (tid + j) * 0x9e3779b9u;
-  }
-  x.l[7] &= 0x1fffffff;
-  y.l[7] &= 0x1fffffff;
-  z.l[7] &= 0x1fffffff;
-  w.l[7] &= 0x1fffffff;
-  uint32_t acc = 0;
-  for (unsigned i = 0; i < iters; i++) {
-    if (KIND == 6) {
-      x = fq::sqr(x);
-      z = fq::sqr(z);
-    } else if (KIND == 7) {
-      x = fq::mul_sub_mul(x, y, z, w);
-      z = fq::mul_sub_mul(z, w, x, y);
-    } else if (KIND == 8) {
-      const fe_wide a = fq::mul_wide(x, y);
-      const fe_wide b = fq::mul_wide(z, w);
-#pragma unroll
-      for (int j = 0; j < 8; j++) {
-        x.l[j] ^= a.l[j + 8];
-        z.l[j] ^= b.l[j] & 0x0fffffff;
-      }
-    } else {
-      x = fq::sub(fq::add(x, y), w);
-      z = fq::sub(fq::add(z, w), y);
-    }
-  }
-  sink[tid] = x.l[0] ^ z.l[1] ^ acc;
-}
-
-// kind 10: sixteen independent double-precision FMAs per iteration (the
-// FP64 pipe, a second multiplier beside the integer one); kind 11: the
-// sixteen mad.lo / mad.hi of kind 0 and sixteen FMAs interleaved, counting
-// only the integer multiplies, to see whether the two pipes overlap.
-template <bool MIXED> __global__ void __launch_bounds__(256) dfma_kernel(uint32_t seed, unsigned iters, uint32_t *sink) {
-  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
-  double d[16];
-  const double m = 0.999 + 1e-9 * (seed & 7), c = 0.5 + 1e-9 * (tid & 15);
-#pragma unroll
-  for (int j = 0; j < 16; j++)
-    d[j] = 1.0 + j + 1e-6 * tid;
-  uint32_t lo[8], hi[8];
-  const uint32_t b = seed ^ (tid * 0x9e3779b9u), cc_ = seed + tid;
-#pragma unroll
-  for (int j = 0; j < 8; j++) {
-    lo[j] = tid * (j + 3);
-    hi[j] = tid ^ (j * 0x85ebca6bu);
-  }
-  for (unsigned i = 0; i < iters; i++) {
-#pragma unroll
-    for (int j = 0; j < 16; j++) {
-      d[j] = __fma_rn(d[j], m, c);
-      if (MIXED && (j & 1) == 0) {
-        asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(lo[j / 2]) : "r"(b), "r"(cc_));
-        asm volatile("mad.hi.u32 %0, %0, %1, %2;" : "+r"(hi[j / 2]) : "r"(b), "r"(cc_));
-      }
-    }
-  }
-  double x = 0;
-  uint32_t y = 0;
-#pragma unroll
-  for (int j = 0; j < 16; j++)
-    x += d[j];
-#pragma unroll
-  for (int j = 0; j < 8; j++)
-    y ^= lo[j] ^ hi[j];
-  sink[tid] = (uint32_t)(long long)x ^ y;
-}
-
 // kind 3: XYZZ += affine chain (never the doubling branch: acc = k*G, k >= 2)
 __global__ void __launch_bounds__(128) madd_kernel(unsigned iters, uint32_t *sink) {
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -213,7 +130,7 @@ __global__ void __launch_bounds__(128) madd_kernel(unsigned iters, uint32_t *sin
 } // namespace
 
 extern "C" bc_error msm_b200_measure_mul_throughput(unsigned kind, double *mulops_per_second) {
-  if (!mulops_per_second || kind > 11)
+  if (!mulops_per_second || kind > 4)
     return bc_error_invalid_value;
   int device = 0, sms = 0;
   cudaError_t e = cudaGetDevice(&device);
@@ -221,17 +138,11 @@ extern "C" bc_error msm_b200_measure_mul_throughput(unsigned kind, double *mulop
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   if (e != cudaSuccess)
     return static_cast<bc_error>(e);
-  const bool light = kind < 2 || kind == 4 || kind == 5 || kind == 10 || kind == 11;
+  const bool light = kind < 2 || kind == 4;
   const unsigned threads = light ? 256 : 128;
   const unsigned blocks = light ? sms * 8 : sms * 4;
-  const unsigned iters = light ? 65536 : kind == 2 ? 4096 : kind == 3 ? 1024 : kind == 9 ? 65536 : 4096;
-  const double per_iter = light ? 16.0
-                          : kind == 2 ? 2.0 * 264
-                          : kind == 3 ? 2392.0
-                          : kind == 6 ? 2.0 * 208
-                          : kind == 7 ? 2.0 * 392
-                          : kind == 8 ? 2.0 * 256
-                                      : 4.0;
+  const unsigned iters = light ? 65536 : kind == 2 ? 4096 : 1024;
+  const double per_iter = light ? 16.0 : kind == 2 ? 2.0 * 264 : 2392.0;
   uint32_t *sink = nullptr;
   cudaStream_t stream = nullptr;
   cudaEvent_t start = nullptr, stop = nullptr;
@@ -250,14 +161,7 @@ extern "C" bc_error msm_b200_measure_mul_throughput(unsigned kind, double *mulop
       case 0: mad_peak_kernel<<<blocks, threads, 0, stream>>>(0x1234567u, iters, sink); break;
       case 1: mad_chain_kernel<<<blocks, threads, 0, stream>>>(0x1234567u, iters, sink); break;
       case 2: montmul_kernel<<<blocks, threads, 0, stream>>>(0x1234567u, iters, sink); break;
-      case 4: mad_half_kernel<false><<<blocks, threads, 0, stream>>>(0x1234567u, iters, sink); break;
-      case 5: mad_half_kernel<true><<<blocks, threads, 0, stream>>>(0x1234567u, iters, sink); break;
-      case 6: component_kernel<6><<<blocks, threads, 0, stream>>>(0x1234567u, iters, sink); break;
-      case 7: component_kernel<7><<<blocks, threads, 0, stream>>>(0x1234567u, iters, sink); break;
-      case 8: component_kernel<8><<<blocks, threads, 0, stream>>>(0x1234567u, iters, sink); break;
-      case 9: component_kernel<9><<<blocks, threads, 0, stream>>>(0x1234567u, iters, sink); break;
-      case 10: dfma_kernel<false><<<blocks, threads, 0, stream>>>(0x1234567u, iters, sink); break;
-      case 11: dfma_kernel<true><<<blocks, threads, 0, stream>>>(0x1234567u, iters, sink); break;
+      case 4: mad_lo_kernel<<<blocks, threads, 0, stream>>>(0x1234567u, iters, sink); break;
       default: madd_kernel<<<blocks, threads, 0, stream>>>(iters, sink); break;
       }
       if ((e = cudaGetLastError()) != cudaSuccess)

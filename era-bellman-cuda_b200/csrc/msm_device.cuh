@@ -218,9 +218,6 @@ __device__ __forceinline__ void sort_scan_row(uint32_t *r, unsigned len, uint32_
 // bit of d.  Measured on a B200, the nine ballots beat __match_any_sync (the
 // stable scatter of a 2^22 MSM: sort stage 1.29 -> 1.19 ms).
 __device__ __forceinline__ unsigned warp_peers(unsigned d) {
-#if defined(SORT_PEERS_BY_MATCH)
-  return __match_any_sync(0xffffffffu, d);
-#else
   unsigned peers = 0xffffffffu;
 #pragma unroll
   for (unsigned b = 0; b <= SORT_RADIX_BITS; b++) {
@@ -229,7 +226,6 @@ __device__ __forceinline__ unsigned warp_peers(unsigned d) {
     peers &= bit ? v : ~v;
   }
   return peers;
-#endif
 }
 
 // Exclusive block-wide scan of 256 shared counters by the first 256 threads.

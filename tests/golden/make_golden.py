@@ -1,7 +1,8 @@
 """Generates the committed golden fixtures in tests/golden/.
 
-Run in a container that has the reference source tree (default
-/root/reference) and the reference host build (make -C oracle ref):
+Run where the reference source tree exists (its path as the first argument,
+else the REF environment variable, else a `reference` directory beside this
+repository) and the reference host build (make -C oracle ref REF=...):
 
     python tests/golden/make_golden.py [/path/to/era-bellman-cuda]
 
@@ -133,4 +134,5 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    repo = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    main(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("REF") or os.path.join(os.path.dirname(repo), "reference"))

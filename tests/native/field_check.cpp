@@ -61,17 +61,16 @@ void fc_fq_mul_sub_mul(const uint32_t *a, const uint32_t *b, const uint32_t *c, 
 
 int fc_fq_is_zero(const uint32_t *a) { return fq::is_zero(ld<fe>(a)) ? 1 : 0; }
 
-// 512-bit products (kind 0: schoolbook mul_wide, 1: Karatsuba, 2: sqr_wide) and
-// Montgomery products (kind 3: CIOS, 4: Karatsuba + REDC)
+// 512-bit products (kind 0: schoolbook mul_wide, 2: sqr_wide) and Montgomery
+// products (kind 3: CIOS, 5: sqr as mul_wide + REDC)
 void fc_fq_wide(int kind, const uint32_t *a, const uint32_t *b, uint32_t *out, int n) {
   for (int i = 0; i < n; i++) {
     const fe x = ld<fe>(a + 8 * i), y = ld<fe>(b + 8 * i);
     switch (kind) {
     case 0: st(out + 16 * i, fq::mul_wide(x, y)); break;
-    case 1: st(out + 16 * i, fq::mul_wide_karatsuba(x, y)); break;
     case 2: st(out + 16 * i, fq::sqr_wide(x)); break;
     case 3: st(out + 8 * i, fq::mul_cios(x, y)); break;
-    case 4: st(out + 8 * i, fq::redc_wide(fq::mul_wide_karatsuba(x, y))); break;
+    case 5: st(out + 8 * i, fq::sqr(x)); break;
     }
   }
 }

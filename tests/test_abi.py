@@ -10,7 +10,9 @@ import pytest
 
 REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 INCLUDE = os.path.join(REPO, "include")
-REF_HEADER = "/root/reference/src/bellman-cuda.h"
+# the reference source tree: the REF environment variable, else a `reference`
+# directory beside this repository (absent on machines without it: skipped)
+REF_HEADER = os.path.join(os.environ.get("REF") or os.path.join(os.path.dirname(REPO), "reference"), "src", "bellman-cuda.h")
 
 
 def declared_functions():
