@@ -7,9 +7,13 @@
 #include "bellman-cuda-b200.h"
 #include "bellman-cuda.h"
 #include "bn254_curve.cuh"
+#include "pointer_access.h"
 
+#include <algorithm>
 #include <cstdint>
 #include <mutex>
+#include <utility>
+#include <vector>
 
 namespace {
 
@@ -18,7 +22,30 @@ inline cudaStream_t S(bc_stream s) { return static_cast<cudaStream_t>(s.handle);
 inline cudaEvent_t E(bc_event e) { return static_cast<cudaEvent_t>(e.handle); }
 inline cudaMemPool_t P(bc_mem_pool p) { return static_cast<cudaMemPool_t>(p.handle); }
 
+// (current device, peer) pairs with peer access enabled through
+// bc_device_enable_peer_access and not disabled since.
+std::mutex peer_lock;
+std::vector<std::pair<int, int>> peer_pairs;
+
+void record_peer_access(int peer, bool enabled) {
+  int current = 0;
+  if (cudaGetDevice(&current) != cudaSuccess)
+    return;
+  std::lock_guard<std::mutex> guard(peer_lock);
+  const auto pair = std::make_pair(current, peer);
+  const auto it = std::find(peer_pairs.begin(), peer_pairs.end(), pair);
+  if (enabled && it == peer_pairs.end())
+    peer_pairs.push_back(pair);
+  if (!enabled && it != peer_pairs.end())
+    peer_pairs.erase(it);
+}
+
 } // namespace
+
+bool msm_b200::peer_access_recorded(int from, int peer) {
+  std::lock_guard<std::mutex> guard(peer_lock);
+  return std::find(peer_pairs.begin(), peer_pairs.end(), std::make_pair(from, peer)) != peer_pairs.end();
+}
 
 extern "C" {
 
@@ -71,8 +98,21 @@ bc_error bc_free(void *ptr) { return to_bc(cudaFree(ptr)); }
 bc_error bc_free_host(void *ptr) { return to_bc(cudaFreeHost(ptr)); }
 bc_error bc_host_register(void *ptr, size_t size) { return to_bc(cudaHostRegister(ptr, size, cudaHostRegisterDefault)); }
 bc_error bc_host_unregister(void *ptr) { return to_bc(cudaHostUnregister(ptr)); }
-bc_error bc_device_disable_peer_access(int device_id) { return to_bc(cudaDeviceDisablePeerAccess(device_id)); }
-bc_error bc_device_enable_peer_access(int device_id) { return to_bc(cudaDeviceEnablePeerAccess(device_id, 0)); }
+// The peer-access wrappers also keep the record that the kernels' pointer
+// checks consult (pointer_access.h): memory of another device is accepted only
+// while the current device has peer access to it.
+bc_error bc_device_disable_peer_access(int device_id) {
+  const cudaError_t e = cudaDeviceDisablePeerAccess(device_id);
+  if (e == cudaSuccess || e == cudaErrorPeerAccessNotEnabled)
+    record_peer_access(device_id, false);
+  return to_bc(e);
+}
+bc_error bc_device_enable_peer_access(int device_id) {
+  const cudaError_t e = cudaDeviceEnablePeerAccess(device_id, 0);
+  if (e == cudaSuccess || e == cudaErrorPeerAccessAlreadyEnabled)
+    record_peer_access(device_id, true);
+  return to_bc(e);
+}
 bc_error bc_memcpy(void *dst, const void *src, size_t count) { return to_bc(cudaMemcpy(dst, src, count, cudaMemcpyDefault)); }
 bc_error bc_memcpy_async(void *dst, const void *src, size_t count, bc_stream stream) {
   return to_bc(cudaMemcpyAsync(dst, src, count, cudaMemcpyDefault, S(stream)));

@@ -15,6 +15,7 @@
 // 254 squarings).
 #include "bellman-cuda-b200.h"
 #include "msm_device.cuh"
+#include "pointer_access.h"
 
 #include <cuda_runtime.h>
 
@@ -115,26 +116,19 @@ __global__ void __launch_bounds__(FINAL_THREADS) final_sum_kernel(const jacobian
   }
 }
 
-// A pointer the kernel can dereference: device or managed memory as is,
-// pinned host memory through its device alias; pageable memory is refused.
+// A pointer the kernel can dereference (pointer_access.h): device memory of
+// the current device or of a peer it has access to, managed memory, or pinned
+// host memory through its device alias; anything else is refused.
 static cudaError_t device_view(const void *ptr, void **view) {
-  cudaPointerAttributes attr{};
-  const cudaError_t err = cudaPointerGetAttributes(&attr, ptr);
+  int device = 0;
+  cudaError_t err = cudaGetDevice(&device);
   if (err != cudaSuccess)
     return err;
-  switch (attr.type) {
-  case cudaMemoryTypeDevice:
-  case cudaMemoryTypeManaged:
-    *view = const_cast<void *>(ptr);
-    return cudaSuccess;
-  case cudaMemoryTypeHost:
-    if (!attr.devicePointer)
-      return cudaErrorInvalidValue;
-    *view = attr.devicePointer;
-    return cudaSuccess;
-  default:
-    return cudaErrorInvalidValue;
-  }
+  cudaPointerAttributes attr{};
+  if ((err = cudaPointerGetAttributes(&attr, ptr)) != cudaSuccess)
+    return err;
+  const bool peer = attr.type == cudaMemoryTypeDevice && attr.device != device && peer_access_recorded(device, attr.device);
+  return kernel_view(ptr, attr, device, peer, host_memory::device_alias, view);
 }
 
 cudaError_t final_sum(const void *results, msm_b200_affine_point *point, cudaStream_t stream) {

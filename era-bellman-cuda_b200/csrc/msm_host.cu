@@ -8,8 +8,11 @@
 #include "bellman-cuda.h"
 #include "bellman-cuda-b200.h"
 #include "msm_host.cuh"
+
+#include <cuda.h> // driver types of the context lookup (no driver calls are linked)
 #include "msm_kernels.cuh"
 #include "plain_tuning.h"
+#include "pointer_access.h"
 
 #include <algorithm>
 #include <cstdlib>
@@ -118,24 +121,33 @@ plan make_plan(unsigned n, unsigned window_bits, int sms) {
 // (no second bucket set, no fold kernel) measured slower: 13.02 against
 // 12.85 ms at 2^22, 25.2 against 23.4 ms at 2^23.  Reference counterpart: the
 // chunked copy/compute overlap of schedule_execution (src/msm.cu:160-334).
-#ifndef MSM_MAX_CHUNKS
-#define MSM_MAX_CHUNKS 4
-#endif
-#ifndef MSM_CHUNK_GROWTH
-#define MSM_CHUNK_GROWTH 5
-#endif
-constexpr unsigned MAX_CHUNKS = MSM_MAX_CHUNKS;
-constexpr unsigned CHUNK_GROWTH = MSM_CHUNK_GROWTH;
+constexpr unsigned MAX_CHUNKS = 4;
+constexpr unsigned CHUNK_GROWTH = 5;
 constexpr double COPY_US_PER_POINT = 0.58e-3; // 32 B scalar over PCIe
-#ifndef MSM_EXTRA_CHUNK_US
-#define MSM_EXTRA_CHUNK_US 360.0
-#endif
-constexpr double EXTRA_CHUNK_US = MSM_EXTRA_CHUNK_US; // one bucket fold + one more pipeline start
+constexpr double EXTRA_CHUNK_US = 360.0;      // one bucket fold + one more pipeline start
 constexpr unsigned MIN_FIRST_CHUNK = 1u << 16;
+// Smallest chunk the out-of-memory fit goes down to (the reference stops at
+// get_log_min_inputs_count, src/msm.cu:39-57, e.g. 2^19 points at 2^22).
+constexpr unsigned MIN_FIT_CHUNK = 1u << 16;
 
+// Chunk boundaries: chunk j holds points [beg[j], beg[j + 1]).  `slots` = 0:
+// copies of host-resident inputs go to a copy area of all n points (chunk j at
+// offset beg[j]); slots = 2: to two chunk-sized slots used in turn (chunk j in
+// slot j & 1), which the out-of-memory fit uses so that the copy area shrinks
+// with the chunks.
 struct chunking {
   unsigned count = 1;
-  unsigned beg[MAX_CHUNKS + 1] = {};
+  unsigned slots = 0;
+  std::vector<unsigned> beg;
+  unsigned size(unsigned j) const { return beg[j + 1] - beg[j]; }
+  unsigned largest() const {
+    unsigned m = 0;
+    for (unsigned j = 0; j < count; j++)
+      m = std::max(m, size(j));
+    return m;
+  }
+  // offset of chunk j in a copy area
+  size_t slot_offset(unsigned j) const { return slots ? (size_t)(j % slots) * largest() : beg[j]; }
 };
 
 static chunking make_chunks(unsigned n, bool copy_inputs) {
@@ -158,6 +170,7 @@ static chunking make_chunks(unsigned n, bool copy_inputs) {
     }
   }
   ch.count = k;
+  ch.beg.resize(k + 1);
   unsigned long long total = 0, weight = 1;
   for (unsigned j = 0; j < k; j++, weight *= CHUNK_GROWTH)
     total += weight;
@@ -171,10 +184,23 @@ static chunking make_chunks(unsigned n, bool copy_inputs) {
   return ch;
 }
 
+// Equal chunks of at most max_chunk points (the out-of-memory fit); host
+// inputs then go through two chunk-sized copy slots.
+static chunking equal_chunks(unsigned n, unsigned max_chunk, bool copy_inputs) {
+  chunking ch;
+  ch.count = (unsigned)(((unsigned long long)n + max_chunk - 1) / max_chunk);
+  ch.slots = copy_inputs && ch.count > 1 ? 2 : 0;
+  ch.beg.resize(ch.count + 1);
+  for (unsigned j = 0; j <= ch.count; j++)
+    ch.beg[j] = (unsigned)((unsigned long long)n * j / ch.count);
+  return ch;
+}
+
 // Scratch layout inside one pool allocation.  `p` is the plan of the largest
 // chunk (keys, values and heads are reused chunk after chunk); copies of
-// host-resident inputs are sized for all `copy_n` points; a chunked MSM holds a
-// second bucket set for the chunks after the first.
+// host-resident inputs are sized for `copy_n` points (all of them, or two
+// chunk slots); a chunked MSM holds a second bucket set for the chunks after
+// the first.
 struct layout {
   size_t keys[2], vals[2], counts, totals, zeros, buckets, flags, chunk_buckets, chunk_flags, hb[2], hp[2], work, tree[2], streams[2], results,
       scalars, bases, total;
@@ -227,26 +253,36 @@ static layout make_layout(const plan &p, bool copy_scalars, bool copy_bases, boo
 // width of the whole MSM.
 static plan largest_chunk_plan(unsigned n, unsigned window_bits, int sms, const chunking &ch) {
   const unsigned c = window_bits ? window_bits : default_window_bits(n);
-  unsigned largest = 0;
-  for (unsigned j = 0; j < ch.count; j++)
-    largest = std::max(largest, ch.beg[j + 1] - ch.beg[j]);
-  return make_plan(largest, c, sms);
+  return make_plan(ch.largest(), c, sms);
+}
+
+// Layout of an MSM split as `ch`.
+static layout chunked_layout(unsigned n, unsigned window_bits, int sms, const chunking &ch, bool copy_scalars, bool copy_bases, bool copy_results) {
+  const plan p = largest_chunk_plan(n, window_bits, sms, ch);
+  const unsigned copy_n = ch.slots ? ch.slots * ch.largest() : n;
+  return make_layout(p, copy_scalars, copy_bases, copy_results, copy_n, ch.count > 1);
 }
 
 size_t scratch_bytes(unsigned n, unsigned window_bits, bool copy_scalars, bool copy_bases, bool copy_results) {
   int device = 0;
   cudaGetDevice(&device);
   const chunking ch = make_chunks(n, copy_scalars || copy_bases);
-  const plan p = largest_chunk_plan(n, window_bits, get_device_info(device).sms, ch);
-  return make_layout(p, copy_scalars, copy_bases, copy_results, n, ch.count > 1).total;
+  return chunked_layout(n, window_bits, get_device_info(device).sms, ch, copy_scalars, copy_bases, copy_results).total;
 }
 
-static bool is_host_pointer(const void *ptr, cudaError_t &err) {
+// Where one of the caller's buffers lives: host memory (pinned or pageable,
+// copied in or out by the call: *host = true) or memory the kernels use in
+// place.  Device memory of another device is refused unless the current
+// device has peer access to it (pointer_access.h): a kernel would fault on it.
+static cudaError_t locate(const void *ptr, int device, bool *host) {
   cudaPointerAttributes attr{};
-  err = cudaPointerGetAttributes(&attr, ptr);
-  if (err != cudaSuccess)
-    return false;
-  return attr.type == cudaMemoryTypeUnregistered || attr.type == cudaMemoryTypeHost;
+  CHECK(cudaPointerGetAttributes(&attr, ptr));
+  *host = attr.type == cudaMemoryTypeUnregistered || attr.type == cudaMemoryTypeHost;
+  if (*host)
+    return cudaSuccess;
+  void *view = nullptr;
+  const bool peer = attr.type == cudaMemoryTypeDevice && attr.device != device && peer_access_recorded(device, attr.device);
+  return kernel_view(ptr, attr, device, peer, host_memory::refuse, &view);
 }
 
 // Stage boundaries: optional caller events recorded before the first stage and
@@ -429,11 +465,13 @@ static cudaError_t collect_profile(const plan &p, const layout &l, const uint8_t
 // work completes).
 struct chunk_resources {
   cudaStream_t copy_stream = nullptr;
-  cudaEvent_t ready = nullptr, copied[MAX_CHUNKS] = {}, copies_done = nullptr;
+  cudaEvent_t ready = nullptr, copies_done = nullptr;
+  std::vector<cudaEvent_t> copied, consumed;
   ~chunk_resources() {
-    for (cudaEvent_t e : copied)
-      if (e)
-        cudaEventDestroy(e);
+    for (const std::vector<cudaEvent_t> *v : {&copied, &consumed})
+      for (cudaEvent_t e : *v)
+        if (e)
+          cudaEventDestroy(e);
     if (ready)
       cudaEventDestroy(ready);
     if (copies_done)
@@ -443,27 +481,44 @@ struct chunk_resources {
   }
 };
 
-// A chunked MSM over host-resident scalars and/or bases (see make_chunks).
+// A chunked MSM: host-resident inputs (see make_chunks), or any inputs whose
+// whole-size scratch did not fit (the out-of-memory fit in execute).  Chunk 0
+// accumulates into the MSM's buckets, every later chunk into a second bucket
+// set that is folded in; the reduction runs once.  With host inputs, copy j + 1
+// runs on a helper stream while chunk j computes; with two copy slots
+// (ch.slots), the copy into a slot also waits until the chunk that used the
+// slot before has finished reading it.
 static cudaError_t enqueue_chunked(const execution &e, const chunking &ch, const plan &full, unsigned sms, bool copy_scalars, bool copy_bases,
                                    jacobian *device_results, uint8_t *scratch, const layout &l) {
   cudaStream_t stream = e.stream;
+  const bool copying = copy_scalars || copy_bases;
   chunk_resources r;
-  CHECK(cudaStreamCreateWithFlags(&r.copy_stream, cudaStreamNonBlocking));
-  CHECK(cudaEventCreateWithFlags(&r.ready, cudaEventDisableTiming));
-  CHECK(cudaEventCreateWithFlags(&r.copies_done, cudaEventDisableTiming));
-  for (unsigned j = 0; j < ch.count; j++)
-    CHECK(cudaEventCreateWithFlags(&r.copied[j], cudaEventDisableTiming));
-  // the copies go into scratch allocated in the caller's stream order
-  CHECK(cudaEventRecord(r.ready, stream));
-  CHECK(cudaStreamWaitEvent(r.copy_stream, r.ready, 0));
   fe *scalars = reinterpret_cast<fe *>(scratch + l.scalars);
   affine *bases = reinterpret_cast<affine *>(scratch + l.bases);
+  if (copying) {
+    CHECK(cudaStreamCreateWithFlags(&r.copy_stream, cudaStreamNonBlocking));
+    CHECK(cudaEventCreateWithFlags(&r.ready, cudaEventDisableTiming));
+    CHECK(cudaEventCreateWithFlags(&r.copies_done, cudaEventDisableTiming));
+    r.copied.assign(ch.count, nullptr);
+    r.consumed.assign(ch.count, nullptr);
+    for (unsigned j = 0; j < ch.count; j++) {
+      CHECK(cudaEventCreateWithFlags(&r.copied[j], cudaEventDisableTiming));
+      if (ch.slots)
+        CHECK(cudaEventCreateWithFlags(&r.consumed[j], cudaEventDisableTiming));
+    }
+    // the copies go into scratch allocated in the caller's stream order
+    CHECK(cudaEventRecord(r.ready, stream));
+    CHECK(cudaStreamWaitEvent(r.copy_stream, r.ready, 0));
+  }
   auto enqueue_copy = [&](unsigned j) -> cudaError_t {
-    const unsigned b = ch.beg[j], cnt = ch.beg[j + 1] - b;
+    const unsigned b = ch.beg[j], cnt = ch.size(j);
+    const size_t at = ch.slot_offset(j);
+    if (ch.slots && j >= ch.slots) // the slot's previous chunk must be done with it
+      CHECK(cudaStreamWaitEvent(r.copy_stream, r.consumed[j - ch.slots], 0));
     if (copy_scalars)
-      CHECK(cudaMemcpyAsync(scalars + b, static_cast<const fe *>(e.scalars) + b, (size_t)cnt * sizeof(fe), cudaMemcpyHostToDevice, r.copy_stream));
+      CHECK(cudaMemcpyAsync(scalars + at, static_cast<const fe *>(e.scalars) + b, (size_t)cnt * sizeof(fe), cudaMemcpyHostToDevice, r.copy_stream));
     if (copy_bases)
-      CHECK(cudaMemcpyAsync(bases + b, static_cast<const affine *>(e.bases) + b, (size_t)cnt * sizeof(affine), cudaMemcpyHostToDevice,
+      CHECK(cudaMemcpyAsync(bases + at, static_cast<const affine *>(e.bases) + b, (size_t)cnt * sizeof(affine), cudaMemcpyHostToDevice,
                             r.copy_stream));
     CHECK(cudaEventRecord(r.copied[j], r.copy_stream));
     if (j + 1 == ch.count) {
@@ -476,8 +531,6 @@ static cudaError_t enqueue_chunked(const execution &e, const chunking &ch, const
     return cudaSuccess;
   };
 
-  const fe *src_scalars = copy_scalars ? scalars : static_cast<const fe *>(e.scalars);
-  const affine *src_bases = copy_bases ? bases : static_cast<const affine *>(e.bases);
   xyzz *buckets = reinterpret_cast<xyzz *>(scratch + l.buckets);
   uint8_t *flags = scratch + l.flags;
   xyzz *chunk_buckets = reinterpret_cast<xyzz *>(scratch + l.chunk_buckets);
@@ -487,27 +540,49 @@ static cudaError_t enqueue_chunked(const execution &e, const chunking &ch, const
   CHECK(cudaMemsetAsync(flags, 0, slots, stream));
   // copy j + 1 is enqueued before chunk j's kernels, so that the host thread
   // (which stages pageable copies itself) never holds back enqueued work
-  CHECK(enqueue_copy(0));
+  if (copying)
+    CHECK(enqueue_copy(0));
   for (unsigned j = 0; j < ch.count; j++) {
-    if (j + 1 < ch.count)
+    if (copying && j + 1 < ch.count)
       CHECK(enqueue_copy(j + 1));
     const unsigned b = ch.beg[j];
-    const plan p = make_plan(ch.beg[j + 1] - b, full.c, sms);
-    CHECK(cudaStreamWaitEvent(stream, r.copied[j], 0));
+    const plan p = make_plan(ch.size(j), full.c, sms);
+    const fe *src_scalars = copy_scalars ? scalars + ch.slot_offset(j) : static_cast<const fe *>(e.scalars) + b;
+    const affine *src_bases = copy_bases ? bases + ch.slot_offset(j) : static_cast<const affine *>(e.bases) + b;
+    if (copying)
+      CHECK(cudaStreamWaitEvent(stream, r.copied[j], 0));
     if (j == 0) {
-      CHECK(enqueue_accumulation(p, src_scalars + b, src_bases + b, buckets, flags, scratch, l, stream, m));
+      CHECK(enqueue_accumulation(p, src_scalars, src_bases, buckets, flags, scratch, l, stream, m));
     } else {
       CHECK(cudaMemsetAsync(chunk_flags, 0, slots, stream));
-      CHECK(enqueue_accumulation(p, src_scalars + b, src_bases + b, chunk_buckets, chunk_flags, scratch, l, stream, m));
+      CHECK(enqueue_accumulation(p, src_scalars, src_bases, chunk_buckets, chunk_flags, scratch, l, stream, m));
       merge_chunk_buckets_kernel<<<(unsigned)((slots + ACC_THREADS - 1) / ACC_THREADS), ACC_THREADS, 0, stream>>>(buckets, flags, chunk_buckets,
                                                                                                                  chunk_flags, (unsigned)slots);
       CHECK(cudaGetLastError());
     }
+    if (copying && ch.slots)
+      CHECK(cudaEventRecord(r.consumed[j], stream));
   }
   CHECK(enqueue_reduction(full, buckets, flags, device_results, scratch, l, stream, m));
   // the call's stream completes after the copies and the h2d callback
-  CHECK(cudaStreamWaitEvent(stream, r.copies_done, 0));
+  if (copying)
+    CHECK(cudaStreamWaitEvent(stream, r.copies_done, 0));
   return cudaSuccess;
+}
+
+// One pool allocation of `bytes` on the call's stream; false with no error
+// when the pool (or the device) cannot hold it, so that the caller can try
+// smaller chunks.  The failed allocation leaves nothing behind; its error is
+// cleared from the runtime's last-error state, as the reference's fit loop
+// does (src/msm.cu:442-446).
+static cudaError_t allocate_scratch(const execution &e, size_t bytes, void **raw, bool *fits) {
+  const cudaError_t err = e.pool ? cudaMallocFromPoolAsync(raw, bytes, e.pool, e.stream) : cudaMallocAsync(raw, bytes, e.stream);
+  *fits = err == cudaSuccess;
+  if (err == cudaErrorMemoryAllocation) {
+    const cudaError_t last = cudaGetLastError();
+    return last == cudaErrorMemoryAllocation ? cudaSuccess : last;
+  }
+  return err;
 }
 
 cudaError_t execute(const execution &e) {
@@ -519,27 +594,36 @@ cudaError_t execute(const execution &e) {
     return cudaErrorInvalidValue;
   int device = 0;
   CHECK(cudaGetDevice(&device));
-  cudaError_t err;
-  const bool copy_scalars = is_host_pointer(e.scalars, err);
-  CHECK(err);
-  const bool copy_bases = is_host_pointer(e.bases, err);
-  CHECK(err);
-  const bool copy_results = is_host_pointer(e.results, err);
-  CHECK(err);
+  bool copy_scalars = false, copy_bases = false, copy_results = false;
+  CHECK(locate(e.scalars, device, &copy_scalars));
+  CHECK(locate(e.bases, device, &copy_bases));
+  CHECK(locate(e.results, device, &copy_results));
   const int sms = get_device_info(device).sms;
   const bool instrumented = e.profile || e.stage_events;
-  const chunking ch = make_chunks(e.count, (copy_scalars || copy_bases) && !instrumented);
   const plan p = make_plan(e.count, e.window_bits, sms);
   if (p.windows > 128)
     return cudaErrorInvalidValue;
-  const plan largest = ch.count > 1 ? largest_chunk_plan(e.count, p.c, sms, ch) : p;
-  const layout l = make_layout(largest, copy_scalars, copy_bases, copy_results, e.count, ch.count > 1);
-  cudaStream_t stream = e.stream;
+  // Memory fit (reference: the dry-run loop of msm::execute_async,
+  // src/msm.cu:431-459): when the pool cannot hold the scratch of the chosen
+  // chunking, the largest chunk is halved -- equal chunks, host inputs through
+  // two chunk-sized copy slots -- down to MIN_FIT_CHUNK points, after which
+  // the call fails with cudaErrorMemoryAllocation.  Device-resident inputs
+  // start as one chunk.  The instrumented entry points run unchunked.
+  chunking ch = make_chunks(e.count, (copy_scalars || copy_bases) && !instrumented);
+  layout l{};
   void *raw = nullptr;
-  if (e.pool)
-    CHECK(cudaMallocFromPoolAsync(&raw, l.total, e.pool, stream));
-  else
-    CHECK(cudaMallocAsync(&raw, l.total, stream));
+  for (;;) {
+    l = chunked_layout(e.count, p.c, sms, ch, copy_scalars, copy_bases, copy_results);
+    bool fits = false;
+    CHECK(allocate_scratch(e, l.total, &raw, &fits));
+    if (fits)
+      break;
+    const unsigned largest = ch.largest();
+    if (instrumented || largest <= MIN_FIT_CHUNK)
+      return cudaErrorMemoryAllocation;
+    ch = equal_chunks(e.count, std::max(MIN_FIT_CHUNK, (largest + 1) / 2), copy_scalars || copy_bases);
+  }
+  cudaStream_t stream = e.stream;
   uint8_t *scratch = static_cast<uint8_t *>(raw);
   cudaError_t status = cudaSuccess;
   do {
@@ -633,22 +717,55 @@ cudaError_t set_up() {
 static_assert(MSM_B200_NO_ALLOC_SCRATCH_BYTES % 256 == 0, "scratch block size");
 static __device__ __align__(256) uint8_t no_alloc_scratch[MSM_B200_NO_ALLOC_SCRATCH_BYTES];
 
-// Device address of no_alloc_scratch on `device` (the current device).  In
-// host code the symbol is only a host-side handle; the address comes from
-// cudaGetSymbolAddress, looked up once per device and cached.
-static cudaError_t no_alloc_scratch_address(int device, uint8_t **address) {
-  static std::mutex lock;
-  static uint8_t *cache[64] = {};
-  if (device < 0 || device >= 64)
-    return cudaErrorInvalidDevice;
-  std::lock_guard<std::mutex> guard(lock);
-  if (!cache[device]) {
-    void *ptr = nullptr;
-    CHECK(cudaGetSymbolAddress(&ptr, no_alloc_scratch));
-    cache[device] = static_cast<uint8_t *>(ptr);
-  }
-  *address = cache[device];
+// Unique id of the calling thread's current CUDA context (cuCtxGetCurrent,
+// cuCtxGetId, reached through the runtime's driver entry points so that the
+// library keeps no link-time dependency on the driver library).
+static cudaError_t current_context_id(unsigned long long *id) {
+  using get_current_fn = CUresult (*)(CUcontext *);
+  using get_id_fn = CUresult (*)(CUcontext, unsigned long long *);
+  static std::once_flag once;
+  static get_current_fn get_current = nullptr;
+  static get_id_fn get_id = nullptr;
+  static cudaError_t resolved = cudaSuccess;
+  std::call_once(once, [] {
+    cudaDriverEntryPointQueryResult found = cudaDriverEntryPointSuccess;
+    void *fn = nullptr;
+    resolved = cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &fn, 12000, cudaEnableDefault, &found);
+    if (resolved == cudaSuccess && found != cudaDriverEntryPointSuccess)
+      resolved = cudaErrorNotSupported;
+    get_current = reinterpret_cast<get_current_fn>(fn);
+    if (resolved == cudaSuccess) {
+      resolved = cudaGetDriverEntryPointByVersion("cuCtxGetId", &fn, 12000, cudaEnableDefault, &found);
+      if (resolved == cudaSuccess && found != cudaDriverEntryPointSuccess)
+        resolved = cudaErrorNotSupported;
+      get_id = reinterpret_cast<get_id_fn>(fn);
+    }
+  });
+  CHECK(resolved);
+  CUcontext ctx = nullptr;
+  if (get_current(&ctx) != CUDA_SUCCESS || !ctx)
+    return cudaErrorIncompatibleDriverContext;
+  if (get_id(ctx, id) != CUDA_SUCCESS)
+    return cudaErrorIncompatibleDriverContext;
   return cudaSuccess;
+}
+
+// Device address of no_alloc_scratch in the current context.  In host code
+// the symbol is only a host-side handle; the address comes from
+// cudaGetSymbolAddress, looked up once per context (each context loads the
+// library's module, and with it the block, at its own address) and cached by
+// the context's unique id, so a reset device or a caller's own context gets
+// its own lookup.
+static cudaError_t no_alloc_scratch_address(uint8_t **address) {
+  static context_cache<uint8_t *> cache;
+  unsigned long long id = 0;
+  CHECK(current_context_id(&id));
+  return cache.get(id, address, [](uint8_t *&ptr) {
+    void *raw = nullptr;
+    const cudaError_t err = cudaGetSymbolAddress(&raw, no_alloc_scratch);
+    ptr = static_cast<uint8_t *>(raw);
+    return err;
+  });
 }
 
 cudaError_t execute_no_alloc(cudaStream_t stream, const void *bases, const void *scalars, void *results, unsigned count) {
@@ -656,21 +773,20 @@ cudaError_t execute_no_alloc(cudaStream_t stream, const void *bases, const void 
     return cudaErrorInvalidValue;
   if ((reinterpret_cast<uintptr_t>(bases) & 15) || (reinterpret_cast<uintptr_t>(scalars) & 15) || (reinterpret_cast<uintptr_t>(results) & 15))
     return cudaErrorInvalidValue;
-  cudaError_t err;
+  int device = 0;
+  CHECK(cudaGetDevice(&device));
   for (const void *ptr : {bases, scalars, static_cast<const void *>(results)}) {
-    const bool host = is_host_pointer(ptr, err);
-    CHECK(err);
+    bool host = false;
+    CHECK(locate(ptr, device, &host));
     if (host)
       return cudaErrorInvalidValue;
   }
-  int device = 0;
-  CHECK(cudaGetDevice(&device));
   const plan p = make_plan(count, 0, get_device_info(device).sms);
   const layout l = make_layout(p, false, false, false);
   if (l.total > MSM_B200_NO_ALLOC_SCRATCH_BYTES) // only on GPUs far larger than a B200 (heads grow with the SM count)
     return cudaErrorInvalidValue;
   uint8_t *scratch = nullptr;
-  CHECK(no_alloc_scratch_address(device, &scratch));
+  CHECK(no_alloc_scratch_address(&scratch));
   return enqueue_pipeline(p, static_cast<const fe *>(scalars), static_cast<const affine *>(bases), static_cast<jacobian *>(results), scratch, l,
                           stream);
 }

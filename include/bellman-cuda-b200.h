@@ -56,13 +56,7 @@ bc_error msm_b200_execute_staged_async(const msm_b200_configuration *configurati
  *   kind 1: carry chains of madc.lo.cc / madc.hi.cc pairs
  *   kind 2: Fq Montgomery products (264 multiply instructions each)
  *   kind 3: XYZZ + affine mixed additions (2392 multiply instructions each)
- *   kind 4: independent mad.lo only;  kind 5: independent mad.hi only
- *   kinds 6..9: squaring, a*b - c*d, 512-bit products, add/sub pairs (the
- *   last reports field additions per second, not multiply instructions)
- *   kind 10: independent double-precision FMAs (FMAs per second)
- *   kind 11: kind 0's integer multiplies interleaved with as many FMAs
- *   (integer multiply instructions per second: equal to kind 0 when the
- *   FP64 pipe runs beside the integer one)
+ *   kind 4: independent mad.lo only
  * Synchronous; about 0.1 s. */
 bc_error msm_b200_measure_mul_throughput(unsigned kind, double *mulops_per_second);
 
@@ -189,9 +183,12 @@ bc_error msm_b200_server_destroy(msm_b200_server server);
  * null or host pointer, or a misaligned buffer returns bc_error_invalid_value
  * before anything is enqueued.  The window width is the size-based default.
  *
- * The first call on a device looks up the block's device address (once per
- * device, with that device current); make that first call before any stream
- * capture.  Every call shares the one block and the block keeps the last
+ * The first call in a CUDA context looks up the block's device address in
+ * that context (cudaGetSymbolAddress, cached by the context's unique id, so a
+ * device reset or a caller's own context gets a fresh lookup); make that
+ * first call before any stream capture.  Device memory of another device is
+ * refused unless peer access to it was enabled through
+ * bc_device_enable_peer_access.  Every call shares the one block and the block keeps the last
  * call's contents (whatever must start at zero is cleared by each call): two
  * calls whose work overlaps on the GPU, on different streams or from
  * different threads, race and both results are undefined.  Serialise them,
@@ -213,10 +210,12 @@ bc_error msm_b200_execute_no_alloc_async(bc_stream stream, const void *bases, co
  * window split produced the R_i.
  *
  * `results` (16-byte aligned) and `point` must be device memory of the
- * current device (or memory it can reach) or pinned host memory (registered
- * or cudaMallocHost'd; the kernel reads and writes it in place); a null or
- * pageable pointer returns bc_error_invalid_value before anything is
- * enqueued.  Asynchronous on `stream`, one kernel of one block, no
+ * current device, device memory of another device to which the current one
+ * has peer access enabled through bc_device_enable_peer_access, managed
+ * memory, or pinned host memory (registered or cudaMallocHost'd; the kernel
+ * reads and writes it in place); a null or pageable pointer, or another
+ * device's memory without that peer access, returns bc_error_invalid_value
+ * before anything is enqueued.  Asynchronous on `stream`, one kernel of one block, no
  * allocation.  Enqueue it after the MSM on the same stream. */
 typedef struct msm_b200_affine_point {
   uint32_t x[8];

@@ -140,6 +140,14 @@ typedef struct msm_configuration {
  *     sum = R_253;  for i = 252 .. 0:  sum = 2 * sum + R_i.
  * Only that sum is defined: the individual R_i depend on the window split.
  * Jacobian infinity is (0, 1, 0) in Montgomery form.
+ *
+ * Scratch comes from configuration.mem_pool in stream order.  When the pool
+ * cannot hold the scratch of the whole MSM, the points are processed in
+ * smaller equal chunks (halved until they fit, down to 2^16 points), as the
+ * reference's dry-run fit does (src/msm.cu:431-459); bc_error_memory_allocation
+ * only when even that does not fit.  Device memory of another device is
+ * refused (bc_error_invalid_value) unless peer access to it was enabled
+ * through bc_device_enable_peer_access.
  */
 bc_error msm_execute_async(msm_configuration configuration);
 
