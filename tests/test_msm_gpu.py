@@ -349,3 +349,88 @@ def test_reference_parity_2_22(gpu, ref_gpu, oracle, dist):
     gpu.bc.free(bd)
     theirs = oracle.horner(ref_gpu.msm(bases, scalars))
     assert ours == theirs
+
+
+# ---- memory fit (reference src/msm.cu:431-459) and large device-resident sizes ----
+def limited_pool(device: int, max_bytes: int):
+    """A memory pool that can hold at most max_bytes (cudaMemPoolProps.maxSize),
+    made through cuda-python; returns (bc_mem_pool handle, destroy function)."""
+    rt = pytest.importorskip("cuda.bindings.runtime")
+    import bellman_cuda as bcm
+    props = rt.cudaMemPoolProps()
+    props.allocType = rt.cudaMemAllocationType.cudaMemAllocationTypePinned
+    props.location.type = rt.cudaMemLocationType.cudaMemLocationTypeDevice
+    props.location.id = device
+    props.maxSize = max_bytes
+    err, pool = rt.cudaMemPoolCreate(props)
+    assert err == rt.cudaError_t.cudaSuccess, err
+    handle = bcm.Handle()
+    handle.handle = int(pool)
+    return handle, lambda: rt.cudaMemPoolDestroy(pool)
+
+
+@pytest.mark.parametrize("scalars_mem", ["device", "pinned"])
+def test_memory_fit_in_a_small_pool(gpu, oracle, scalars_mem):
+    """A pool that cannot hold the whole-size scratch of a 2^22 MSM (half of it):
+    the call runs in smaller chunks instead of failing, device-resident or
+    host-resident scalars alike, bit-exact; a pool too small for even the
+    smallest chunk gives bc_error_memory_allocation (nothing enqueued)."""
+    import bellman_cuda as bcm
+    bc = gpu.bc
+    n = 1 << 22
+    full = bc.scratch_bytes(n)
+    scalars, k = synth.workload("skewed" if scalars_mem == "device" else "uniform", n, 231)
+    bd, _ = generated_bases(gpu, k)
+    rd = bc.malloc(254 * 96)
+    owned, pinned = [], []
+    if scalars_mem == "device":
+        sd = gpu.upload(scalars)
+        owned.append(sd)
+    else:
+        hs, sd = bc.pinned_array(scalars.shape)
+        hs[...] = scalars
+        pinned.append(sd)
+    pool, destroy = limited_pool(0, full // 2)
+    try:
+        assert bc.msm_execute_async(pool, gpu.stream, bd, sd, rd, 22) == bcm.BC_SUCCESS
+        bc.stream_synchronize(gpu.stream)
+        assert oracle.horner(bc.from_device(rd, (254, 24))) == oracle.msm_checksum(k, scalars)
+    finally:
+        destroy()
+    tiny, destroy_tiny = limited_pool(0, 32 << 20)
+    try:
+        assert bc.msm_execute_async(tiny, gpu.stream, bd, sd, rd, 22) == bcm.BC_ERROR_MEMORY_ALLOCATION
+        bc.stream_synchronize(gpu.stream)
+    finally:
+        destroy_tiny()
+    for p in owned + [bd, rd]:
+        bc.free(p)
+    for p in pinned:
+        bc.free_host(p)
+
+
+@pytest.mark.parametrize("log_n", [24, 26])
+def test_device_resident_large(gpu, oracle, log_n):
+    """Device-resident MSMs past 2^22 (the reference tests and benchmarks up to
+    2^26, tests/msm_test.cu:253-260): every window stride and entry index past
+    2^31 entries, against the checksum oracle."""
+    n = 1 << log_n
+    scalars, k = synth.workload("skewed" if log_n == 24 else "uniform", n, 240 + log_n)
+    kd = gpu.upload(k)
+    bd = gpu.bc.malloc(n * 64)
+    gpu.bc.generator_multiples(kd, bd, n, gpu.stream)
+    gpu.bc.stream_synchronize(gpu.stream)
+    gpu.bc.free(kd)
+    res = gpu.msm(None, scalars, bases_dev=bd)
+    gpu.bc.free(bd)
+    assert oracle.horner(res) == oracle.msm_checksum(k, scalars)
+
+
+def test_reference_parity_2_24(gpu, ref_gpu, oracle):
+    n = 1 << 24
+    scalars, k = synth.workload("uniform", n, 265)
+    bd, bases = generated_bases(gpu, k)
+    ours = oracle.horner(gpu.msm(None, scalars, bases_dev=bd))
+    gpu.bc.free(bd)
+    theirs = oracle.horner(ref_gpu.msm(bases, scalars))
+    assert ours == theirs == oracle.msm_checksum(k, scalars)
