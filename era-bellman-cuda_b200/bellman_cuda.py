@@ -97,6 +97,7 @@ class MsmB200Profile(ctypes.Structure):
         ("windows", ctypes.c_uint),
         ("acc_threads", ctypes.c_uint),
         ("launches", ctypes.c_uint),
+        ("sort_wait_timeouts", ctypes.c_uint),
     ]
 
     @property

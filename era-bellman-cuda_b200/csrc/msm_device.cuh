@@ -192,7 +192,7 @@ __device__ __forceinline__ void sort_histogram_tile(const uint32_t *__restrict__
 // lane (coalesced: each load and store is one 128-byte line), scanned across
 // the warp with shuffles and offset by the running total.  (Lane-contiguous
 // chunks made every load touch 32 lines; at 2^22 the scan kernel took 57 us.)
-__device__ __forceinline__ void sort_scan_row(uint32_t *r, unsigned len, uint32_t *__restrict__ total) {
+__device__ __forceinline__ void sort_scan_row(uint32_t *r, unsigned len, uint32_t *__restrict__ total, bool write_prefix = true) {
   const unsigned lane = threadIdx.x & 31;
   uint32_t run = 0;
   for (unsigned base = 0; base < len; base += 32) {
@@ -205,7 +205,7 @@ __device__ __forceinline__ void sort_scan_row(uint32_t *r, unsigned len, uint32_
       if (lane >= (unsigned)off)
         incl += u;
     }
-    if (t < len)
+    if (t < len && write_prefix)
       r[t] = run + incl - v;
     run += __shfl_sync(0xffffffffu, incl, 31);
   }
@@ -254,21 +254,24 @@ __device__ __forceinline__ void scan_256(const uint32_t *in, uint32_t *out, uint
   __syncthreads();
 }
 
-// Scatter one tile: `count` items at seg_in + base of a segment whose digit
-// totals are seg_totals[0..255], to seg_out + (digit base + rank);
-// tile_counts[d * count_stride] is this tile's exclusive prefix over the
-// segment's earlier tiles for digit d.  DROP_ZEROS (the first pass): ZERO_KEY
-// entries are not written (the histogram left them out).  Ranks among equal digits: STABLE (every pass after the
-// first, which LSD order requires) ranks warp by warp, 32 consecutive items
-// per round with warp_peers (ballots); the first pass may take any order and
-// ranks with shared atomics.  The tile is then reordered in shared memory so
-// that each digit's run is written to global memory with consecutive
-// addresses.
-template <bool STABLE, bool DROP_ZEROS>
-__device__ __forceinline__ void sort_scatter_tile(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
-                                                  uint32_t *__restrict__ keys_out, uint32_t *__restrict__ vals_out, size_t seg_in, size_t seg_out,
-                                                  unsigned base, unsigned count, unsigned shift, const uint32_t *__restrict__ tile_counts,
-                                                  size_t count_stride, const uint32_t *__restrict__ seg_totals) {
+// Scatter one tile: `count` items at seg_in + base, each to seg_out + (the
+// global position of its digit's run for this tile) + (its rank among the
+// tile's items of that digit).  DROP_ZEROS (the first pass): ZERO_KEY entries
+// are not written (the histograms left them out).  Ranks among equal digits:
+// STABLE (every pass after the first, which LSD order requires) ranks warp by
+// warp, 32 consecutive items per round with warp_peers (ballots); the first
+// pass may take any order and ranks with shared atomics.  The tile is then
+// reordered in shared memory so that each digit's run is written to global
+// memory with consecutive addresses.
+//
+// RUN_BASES fills glob[d] (d < SORT_RADIX), the position of this tile's run
+// of digit d relative to seg_out, from the tile's digit counts tile_cnt[]; it
+// is called by every thread of the block (it may synchronise the block) and
+// may use digit_base[] and warp_sums[] as scratch.
+template <bool STABLE, bool DROP_ZEROS, class RUN_BASES>
+__device__ __forceinline__ void scatter_tile(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in, uint32_t *__restrict__ keys_out,
+                                             uint32_t *__restrict__ vals_out, size_t seg_in, size_t seg_out, unsigned base, unsigned count,
+                                             unsigned shift, RUN_BASES run_bases) {
   __shared__ uint32_t s_key[SORT_TILE];
   __shared__ uint32_t s_val[SORT_TILE];
   __shared__ uint32_t whist[STABLE ? SORT_WARPS : 1][SORT_RADIX];
@@ -324,12 +327,8 @@ __device__ __forceinline__ void sort_scatter_tile(const uint32_t *__restrict__ k
   scan_256(tile_cnt, tile_off, warp_sums);
   if (threadIdx.x == SORT_RADIX - 1)
     staged = tile_off[SORT_RADIX - 1] + tile_cnt[SORT_RADIX - 1]; // items kept (dropped zero keys excluded)
-  for (unsigned d = threadIdx.x; d < SORT_RADIX; d += blockDim.x)
-    glob[d] = seg_totals[d];
+  run_bases(static_cast<const uint32_t *>(tile_cnt), glob, digit_base, warp_sums);
   __syncthreads();
-  scan_256(glob, digit_base, warp_sums); // digit bases of this segment
-  for (unsigned d = threadIdx.x; d < SORT_RADIX; d += blockDim.x)
-    glob[d] = digit_base[d] + tile_counts[d * count_stride];
 #pragma unroll
   for (unsigned r = 0; r < SORT_ITEMS; r++) {
     const unsigned i = sub + r * 32 + lane;
@@ -352,6 +351,138 @@ __device__ __forceinline__ void sort_scatter_tile(const uint32_t *__restrict__ k
       vals_out[out] = s_val[pos];
     }
   }
+}
+
+// Scatter with run positions from a histogram + scan pass (the batched
+// pipeline): seg_totals[0..255] are the segment's digit totals and
+// tile_counts[d * count_stride] this tile's exclusive prefix over the
+// segment's earlier tiles for digit d.
+template <bool STABLE, bool DROP_ZEROS>
+__device__ __forceinline__ void sort_scatter_tile(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
+                                                  uint32_t *__restrict__ keys_out, uint32_t *__restrict__ vals_out, size_t seg_in, size_t seg_out,
+                                                  unsigned base, unsigned count, unsigned shift, const uint32_t *__restrict__ tile_counts,
+                                                  size_t count_stride, const uint32_t *__restrict__ seg_totals) {
+  scatter_tile<STABLE, DROP_ZEROS>(keys_in, vals_in, keys_out, vals_out, seg_in, seg_out, base, count, shift,
+                                   [&](const uint32_t *, uint32_t *glob, uint32_t *digit_base, uint32_t *warp_sums) {
+                                     for (unsigned d = threadIdx.x; d < SORT_RADIX; d += blockDim.x)
+                                       glob[d] = seg_totals[d];
+                                     __syncthreads();
+                                     scan_256(glob, digit_base, warp_sums); // digit bases of this segment
+                                     for (unsigned d = threadIdx.x; d < SORT_RADIX; d += blockDim.x)
+                                       glob[d] = digit_base[d] + tile_counts[d * count_stride];
+                                   });
+}
+
+// ---------------------------------------------------------------------------
+// stable radix passes in one kernel, with decoupled look-back (the plain
+// pipeline's passes after the first)
+// ---------------------------------------------------------------------------
+// Per (window, tile): a flag word -- LOOKBACK_NONE, LOOKBACK_AGGREGATE (the
+// tile's own digit counts are in agg[tile][0..255]) or LOOKBACK_INCLUSIVE (the
+// counts over this and every earlier tile of the window are in
+// incl[tile][0..255]).  The counts are written first and made visible
+// (__threadfence) before the flag is set; readers load the flag with acquire
+// semantics before the counts.
+constexpr uint32_t LOOKBACK_NONE = 0, LOOKBACK_AGGREGATE = 1, LOOKBACK_INCLUSIVE = 2;
+// Polls of a batch of predecessors, one of which has published nothing yet,
+// before a wait gives up (well under a second with the back-off below).  A
+// predecessor took its tile earlier from the same counter, so it is resident
+// and publishes its counts right after ranking: in correct operation the wait
+// ends within microseconds; the limit only keeps a failure from hanging the
+// GPU.
+constexpr unsigned LOOKBACK_MAX_POLLS = 1u << 20;
+constexpr int LOOKBACK_GAVE_UP = -2;
+static_assert(SORT_THREADS == SORT_RADIX, "look-back: one digit per thread");
+
+__device__ __forceinline__ uint32_t load_acquire(const uint32_t *p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ uint32_t load_relaxed(const uint32_t *p) {
+  uint32_t v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void store_release(uint32_t *p, uint32_t v) { asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory"); }
+
+// Publishes this tile's digit counts (all threads call it; one digit per
+// thread) under `flag`.
+__device__ __forceinline__ void lookback_publish(uint32_t *flags, uint32_t *counts, unsigned tile, uint32_t value, uint32_t flag) {
+  counts[(size_t)tile * SORT_RADIX + threadIdx.x] = value;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0)
+    store_release(flags + tile, flag);
+}
+
+// One stable radix pass over one tile of a window segment, with run
+// positions found by decoupled look-back over the window's earlier tiles:
+// after ranking, the tile publishes its aggregate; the first warp then reads
+// the flags of the 32 nearest earlier tiles at a time until it finds one with
+// an inclusive count (waiting, bounded, while a tile between has published
+// nothing), and every thread adds that inclusive count and the aggregates
+// after it for its digit; the tile then publishes its own inclusive count.
+// totals: the window's digit totals.  A wait that gives up sets *error and
+// uses what it has (positions then only shrink, so every write stays inside
+// the segment): the kernel always ends; the sort is wrong and *error says so.
+__device__ __forceinline__ void lookback_tile(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
+                                              uint32_t *__restrict__ keys_out, uint32_t *__restrict__ vals_out, size_t seg, unsigned tile,
+                                              unsigned count, unsigned shift, uint32_t *flags, uint32_t *agg, uint32_t *incl,
+                                              const uint32_t *__restrict__ totals, unsigned *error) {
+  scatter_tile<true, false>(
+      keys_in, vals_in, keys_out, vals_out, seg, seg, tile * SORT_TILE, count, shift,
+      [&](const uint32_t *tile_cnt, uint32_t *glob, uint32_t *digit_base, uint32_t *warp_sums) {
+        __shared__ int s_start;
+        const unsigned d = threadIdx.x, lane = threadIdx.x & 31;
+        const uint32_t own = tile_cnt[d];
+        lookback_publish(flags, agg, tile, own, LOOKBACK_AGGREGATE);
+        if (threadIdx.x < 32) {
+          int hi = (int)tile; // tiles [0, hi) are still to be examined
+          int start = -1;     // nearest earlier tile with an inclusive count
+          unsigned polls = 0;
+          while (hi > 0) {
+            const int j = hi - 1 - (int)lane;
+            const uint32_t f = j >= 0 ? load_acquire(flags + j) : LOOKBACK_AGGREGATE;
+            const unsigned inclusive = __ballot_sync(0xffffffffu, f == LOOKBACK_INCLUSIVE);
+            const unsigned missing = __ballot_sync(0xffffffffu, f == LOOKBACK_NONE);
+            const unsigned nearest = inclusive ? __ffs(inclusive) - 1 : 32;
+            const unsigned before = nearest == 32 ? 0xffffffffu : (1u << nearest) - 1;
+            if (missing & before) {
+              if (++polls == LOOKBACK_MAX_POLLS) {
+                if (lane == 0)
+                  atomicOr(error, 1u);
+                start = LOOKBACK_GAVE_UP;
+                break;
+              }
+              __nanosleep(100);
+              continue;
+            }
+            if (nearest < 32) {
+              start = hi - 1 - (int)nearest;
+              break;
+            }
+            hi -= 32;
+          }
+          if (lane == 0)
+            s_start = start;
+        }
+        glob[d] = totals[d];
+        __syncthreads();
+        scan_256(glob, digit_base, warp_sums); // digit bases of this segment
+        const int start = s_start;
+        uint32_t prefix = start >= 0 ? load_relaxed(incl + (size_t)start * SORT_RADIX + d) : 0;
+        if (start != LOOKBACK_GAVE_UP) {
+          for (int j = start + 1; j < (int)tile; j++)
+            prefix += load_relaxed(agg + (size_t)j * SORT_RADIX + d);
+        } else { // add what the earlier tiles have published
+          for (int j = 0; j < (int)tile; j++)
+            if (load_relaxed(flags + j) != LOOKBACK_NONE)
+              prefix += load_relaxed(agg + (size_t)j * SORT_RADIX + d);
+        }
+        glob[d] = digit_base[d] + prefix;
+        lookback_publish(flags, incl, tile, prefix + own, LOOKBACK_INCLUSIVE);
+      });
 }
 
 // ---------------------------------------------------------------------------

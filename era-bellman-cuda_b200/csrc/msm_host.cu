@@ -84,6 +84,7 @@ unsigned accumulation_ranges(unsigned threads, unsigned long long entries, unsig
 plan make_plan(unsigned n, unsigned window_bits, int sms) {
   plan p{};
   p.n = n;
+  p.sms = (unsigned)sms;
   p.c = window_bits ? window_bits : default_window_bits(n);
   p.windows = (RESULT_BITS + p.c - 1) / p.c;
   p.log_b = p.c - 1;
@@ -129,6 +130,8 @@ constexpr unsigned MIN_FIRST_CHUNK = 1u << 16;
 // Smallest chunk the out-of-memory fit goes down to (the reference stops at
 // get_log_min_inputs_count, src/msm.cu:39-57, e.g. 2^19 points at 2^22).
 constexpr unsigned MIN_FIT_CHUNK = 1u << 16;
+// Largest chunk: the radix passes' look-back words hold counts below 2^30.
+constexpr unsigned MAX_CHUNK_POINTS = 1u << 29;
 
 // Chunk boundaries: chunk j holds points [beg[j], beg[j + 1]).  `slots` = 0:
 // copies of host-resident inputs go to a copy area of all n points (chunk j at
@@ -202,8 +205,8 @@ static chunking equal_chunks(unsigned n, unsigned max_chunk, bool copy_inputs) {
 // chunk slots); a chunked MSM holds a second bucket set for the chunks after
 // the first.
 struct layout {
-  size_t keys[2], vals[2], counts, totals, zeros, buckets, flags, chunk_buckets, chunk_flags, hb[2], hp[2], work, tree[2], streams[2], results,
-      scalars, bases, total;
+  size_t keys[2], vals[2], counts, totals, zeros, sort_ctrs, sort_error, lookback_flags, sort_small_bytes, lookback_agg, lookback_incl, buckets, flags,
+      chunk_buckets, chunk_flags, hb[2], hp[2], work, tree[2], streams[2], results, scalars, bases, total;
 };
 
 static size_t align_up(size_t v) { return (v + 255) & ~(size_t)255; }
@@ -223,9 +226,21 @@ static layout make_layout(const plan &p, bool copy_scalars, bool copy_bases, boo
     l.keys[i] = take(entries * 4);
     l.vals[i] = take(entries * 4);
   }
-  l.counts = take((size_t)p.windows * SORT_RADIX * p.tiles * 4);
-  l.totals = take((size_t)p.windows * SORT_RADIX * 4);
-  l.zeros = take((size_t)p.windows * 4);
+  // digit counts per (pass, window, digit, tile); then one region cleared per
+  // chunk: digit totals per (pass, window, digit), zero digits per window, a
+  // tile counter per pass, the look-back error word and the look-back flags
+  // of the passes after the first; then the look-back counts (shared by those
+  // passes)
+  const size_t lookback_words = (size_t)p.windows * p.tiles;
+  l.counts = take((size_t)p.sort_passes * p.windows * SORT_RADIX * p.tiles * 4);
+  l.sort_small_bytes = ((size_t)p.sort_passes * p.windows * SORT_RADIX + p.windows + p.sort_passes + 1 + (p.sort_passes - 1) * lookback_words) * 4;
+  l.totals = take(l.sort_small_bytes);
+  l.zeros = l.totals + (size_t)p.sort_passes * p.windows * SORT_RADIX * 4;
+  l.sort_ctrs = l.zeros + (size_t)p.windows * 4;
+  l.sort_error = l.sort_ctrs + (size_t)p.sort_passes * 4;
+  l.lookback_flags = l.sort_error + 4;
+  l.lookback_agg = p.sort_passes > 1 ? take(lookback_words * SORT_RADIX * 4) : 0;
+  l.lookback_incl = p.sort_passes > 1 ? take(lookback_words * SORT_RADIX * 4) : 0;
   const size_t slots = (size_t)p.windows << p.log_b;
   l.buckets = take(slots * sizeof(xyzz));
   l.flags = take(slots);
@@ -285,6 +300,21 @@ static cudaError_t locate(const void *ptr, int device, bool *host) {
   return kernel_view(ptr, attr, device, peer, host_memory::refuse, &view);
 }
 
+// Dynamic shared memory of digits_histogram_kernel: a counter per (pass,
+// window, digit) and one per window for zero digits.
+static size_t digit_histogram_smem(unsigned windows, unsigned passes) { return ((size_t)passes * windows * SORT_RADIX + windows) * 4; }
+
+// The largest of those over the window widths that use the kernel.
+static size_t max_digit_histogram_smem() {
+  size_t most = 0;
+  for (unsigned c = 2; c <= 24; c++) {
+    const unsigned windows = (RESULT_BITS + c - 1) / c, passes = (c - 1 + SORT_RADIX_BITS - 1) / SORT_RADIX_BITS;
+    if (windows <= MAX_FUSED_HISTOGRAM_WINDOWS)
+      most = std::max(most, digit_histogram_smem(windows, passes));
+  }
+  return most;
+}
+
 // Stage boundaries: optional caller events recorded before the first stage and
 // after each of the PROFILE_STAGES stages, and a count of kernels enqueued.
 struct stage_marks {
@@ -308,44 +338,67 @@ static cudaError_t enqueue_accumulation(const plan &p, const fe *scalars, const 
   xyzz *hp[2] = {reinterpret_cast<xyzz *>(scratch + l.hp[0]), reinterpret_cast<xyzz *>(scratch + l.hp[1])};
   const unsigned n = p.n;
 
-  // 1. digits (with the first sort pass's histograms when they fit in shared memory)
-  CHECK(cudaMemsetAsync(zeros, 0, p.windows * sizeof(uint32_t), stream));
-  const bool fused_histogram = p.windows <= MAX_FUSED_HISTOGRAM_WINDOWS;
-  if (fused_histogram) {
-    digits_histogram_kernel<<<p.tiles, SORT_THREADS, p.windows * (SORT_RADIX + 1) * 4, stream>>>(scalars, n, p.c, p.windows, p.tiles, keys[0],
-                                                                                                  vals[0], counts, zeros);
-  } else {
-    digits_kernel<<<(n + 255) / 256, 256, 0, stream>>>(scalars, n, p.c, p.windows, keys[0], vals[0]);
-  }
-  CHECK(cudaGetLastError());
-  m.launched++;
-  CHECK(m.mark(stream));
-
-  // 2. sort, 8 bits per pass
+  unsigned *sort_ctrs = reinterpret_cast<unsigned *>(scratch + l.sort_ctrs);
+  unsigned *sort_error = reinterpret_cast<unsigned *>(scratch + l.sort_error);
+  CHECK(cudaMemsetAsync(totals, 0, l.sort_small_bytes, stream));
   int cur = 0;
-  const unsigned rows = p.windows * SORT_RADIX;
-  for (unsigned pass = 0; pass < p.sort_passes; pass++) {
-    const unsigned shift = pass * SORT_RADIX_BITS;
+  if (p.windows <= MAX_FUSED_HISTOGRAM_WINDOWS) {
+    // 1. digits, with every pass's digit counts per tile
+    digits_histogram_kernel<<<p.tiles, SORT_THREADS, digit_histogram_smem(p.windows, p.sort_passes), stream>>>(
+        scalars, n, p.c, p.windows, p.sort_passes, p.tiles, keys[0], vals[0], counts, zeros);
+    CHECK(cudaGetLastError());
+    m.launched++;
+    CHECK(m.mark(stream));
+    // 2. sort: one scan for the first pass's tile offsets and every pass's
+    // digit totals, the first pass (drops zero digits), then one look-back
+    // kernel per later 8-bit pass
+    const unsigned prefix_rows = p.windows * SORT_RADIX, rows = p.sort_passes * prefix_rows;
+    sort_scan_kernel<<<(rows * 32 + 255) / 256, 256, 0, stream>>>(counts, p.tiles, rows, totals, prefix_rows);
+    CHECK(cudaGetLastError());
     const dim3 grid(p.tiles, p.windows);
-    if (pass > 0 || !fused_histogram) {
+    sort_scatter_first_kernel<<<grid, SORT_THREADS, 0, stream>>>(keys[0], vals[0], keys[1], vals[1], n, p.tiles, 0, counts, totals, zeros);
+    CHECK(cudaGetLastError());
+    m.launched += 2;
+    cur = 1;
+    uint32_t *lookback_flags = reinterpret_cast<uint32_t *>(scratch + l.lookback_flags);
+    uint32_t *agg = reinterpret_cast<uint32_t *>(scratch + l.lookback_agg), *incl = reinterpret_cast<uint32_t *>(scratch + l.lookback_incl);
+    for (unsigned pass = 1; pass < p.sort_passes; pass++) {
+      lookback_stable_kernel<<<p.windows * p.tiles, SORT_THREADS, 0, stream>>>(
+          keys[cur], vals[cur], keys[cur ^ 1], vals[cur ^ 1], n, p.windows, p.tiles, pass * SORT_RADIX_BITS,
+          lookback_flags + (size_t)(pass - 1) * p.windows * p.tiles, agg, incl, totals + (size_t)pass * prefix_rows, zeros, sort_ctrs + pass,
+          sort_error);
+      CHECK(cudaGetLastError());
+      m.launched++;
+      cur ^= 1;
+    }
+  } else {
+    // 1. digits (c <= 5: more windows than the digit kernel can count)
+    digits_kernel<<<(n + 255) / 256, 256, 0, stream>>>(scalars, n, p.c, p.windows, keys[0], vals[0]);
+    CHECK(cudaGetLastError());
+    m.launched++;
+    CHECK(m.mark(stream));
+    // 2. sort, 8 bits per pass: histogram, scan and scatter kernels
+    const unsigned rows = p.windows * SORT_RADIX;
+    for (unsigned pass = 0; pass < p.sort_passes; pass++) {
+      const unsigned shift = pass * SORT_RADIX_BITS;
+      const dim3 grid(p.tiles, p.windows);
       if (pass == 0)
         sort_histogram_first_kernel<<<grid, SORT_THREADS, 0, stream>>>(keys[cur], n, p.tiles, shift, counts, zeros);
       else
         sort_histogram_kernel<<<grid, SORT_THREADS, 0, stream>>>(keys[cur], n, p.tiles, shift, counts, zeros);
       CHECK(cudaGetLastError());
-      m.launched++;
+      sort_scan_kernel<<<(rows * 32 + 255) / 256, 256, 0, stream>>>(counts, p.tiles, rows, totals, rows);
+      CHECK(cudaGetLastError());
+      if (pass == 0)
+        sort_scatter_first_kernel<<<grid, SORT_THREADS, 0, stream>>>(keys[cur], vals[cur], keys[cur ^ 1], vals[cur ^ 1], n, p.tiles, shift, counts,
+                                                                     totals, zeros);
+      else
+        sort_scatter_stable_kernel<<<grid, SORT_THREADS, 0, stream>>>(keys[cur], vals[cur], keys[cur ^ 1], vals[cur ^ 1], n, p.tiles, shift, counts,
+                                                                      totals, zeros);
+      CHECK(cudaGetLastError());
+      m.launched += 3;
+      cur ^= 1;
     }
-    sort_scan_kernel<<<(rows * 32 + 255) / 256, 256, 0, stream>>>(counts, p.tiles, rows, totals);
-    CHECK(cudaGetLastError());
-    if (pass == 0)
-      sort_scatter_first_kernel<<<grid, SORT_THREADS, 0, stream>>>(keys[cur], vals[cur], keys[cur ^ 1], vals[cur ^ 1], n, p.tiles, shift, counts,
-                                                                   totals, zeros);
-    else
-      sort_scatter_stable_kernel<<<grid, SORT_THREADS, 0, stream>>>(keys[cur], vals[cur], keys[cur ^ 1], vals[cur ^ 1], n, p.tiles, shift, counts,
-                                                                    totals, zeros);
-    CHECK(cudaGetLastError());
-    m.launched += 2;
-    cur ^= 1;
   }
   CHECK(m.mark(stream));
 
@@ -439,6 +492,8 @@ static cudaError_t collect_profile(const plan &p, const layout &l, const uint8_t
     CHECK(cudaEventElapsedTime(&out->stage_ms[s], events[s], events[s + 1]));
   std::vector<uint32_t> zeros(p.windows);
   CHECK(cudaMemcpy(zeros.data(), scratch + l.zeros, zeros.size() * 4, cudaMemcpyDeviceToHost));
+  uint32_t sort_error = 0;
+  CHECK(cudaMemcpy(&sort_error, scratch + l.sort_error, 4, cudaMemcpyDeviceToHost));
   std::vector<uint8_t> flags((size_t)p.windows << p.log_b);
   CHECK(cudaMemcpy(flags.data(), scratch + l.flags, flags.size(), cudaMemcpyDeviceToHost));
   std::vector<uint32_t> heads(p.acc_ranges);
@@ -457,6 +512,7 @@ static cudaError_t collect_profile(const plan &p, const layout &l, const uint8_t
   out->windows = p.windows;
   out->acc_threads = p.acc_ranges;
   out->launches = launches;
+  out->sort_wait_timeouts = sort_error;
   return cudaSuccess;
 }
 
@@ -610,6 +666,11 @@ cudaError_t execute(const execution &e) {
   // the call fails with cudaErrorMemoryAllocation.  Device-resident inputs
   // start as one chunk.  The instrumented entry points run unchunked.
   chunking ch = make_chunks(e.count, (copy_scalars || copy_bases) && !instrumented);
+  if (ch.largest() > MAX_CHUNK_POINTS) {
+    if (instrumented)
+      return cudaErrorInvalidValue;
+    ch = equal_chunks(e.count, MAX_CHUNK_POINTS, copy_scalars || copy_bases);
+  }
   layout l{};
   void *raw = nullptr;
   for (;;) {
@@ -701,8 +762,7 @@ template <class F> static cudaError_t set_carveout(F *func, int percent) {
 }
 
 cudaError_t set_up() {
-  CHECK(cudaFuncSetAttribute(digits_histogram_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             MAX_FUSED_HISTOGRAM_WINDOWS * (SORT_RADIX + 1) * 4));
+  CHECK(cudaFuncSetAttribute(digits_histogram_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_digit_histogram_smem()));
   CHECK(set_carveout(accumulate_kernel, ACC_CARVEOUT)); // 4 blocks x 19 KB of base-point slots and window bounds
   CHECK(set_carveout(merge_heads_kernel, cudaSharedmemCarveoutMaxL1));
   CHECK(set_carveout(reduce_groups_kernel, cudaSharedmemCarveoutMaxL1));

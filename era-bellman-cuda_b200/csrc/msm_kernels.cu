@@ -16,20 +16,26 @@ __global__ void __launch_bounds__(256) digits_kernel(const fe *__restrict__ scal
   });
 }
 
-// The same, one block per sort tile (SORT_TILE scalars), also producing the
-// first radix pass's tile histograms (low 8 bits of every window's nonzero
-// keys), so that pass needs no histogram kernel, and adding each window's
-// zero digits to zeros[w].  Dynamic shared memory: windows x 257 counters.
+// The same, one block per sort tile (SORT_TILE scalars), also counting the
+// tile's nonzero keys per window and radix digit for every sort pass
+// (dynamic shared memory: passes x windows x 256 counters, then windows zero
+// counters): hist[((p * windows + w) * 256 + d) * tiles + tile] receives the
+// count of digit d of pass p.  sort_scan_kernel turns pass 0's counts into
+// the first radix pass's tile offsets and every pass's into digit totals.
+// Each window's zero digits are added to zeros[w].
 __global__ void __launch_bounds__(SORT_THREADS) digits_histogram_kernel(const fe *__restrict__ scalars, unsigned n, unsigned c, unsigned windows,
-                                                                        unsigned tiles, uint32_t *__restrict__ keys, uint32_t *__restrict__ vals,
-                                                                        uint32_t *__restrict__ counts, uint32_t *__restrict__ zeros) {
-  extern __shared__ uint32_t hist[]; // [windows][SORT_RADIX], then [windows] zero digits
-  uint32_t *zero_digits = hist + windows * SORT_RADIX;
+                                                                        unsigned passes, unsigned tiles, uint32_t *__restrict__ keys,
+                                                                        uint32_t *__restrict__ vals, uint32_t *__restrict__ hist,
+                                                                        uint32_t *__restrict__ zeros) {
+  extern __shared__ uint32_t s_hist[]; // [passes][windows][SORT_RADIX], then [windows] zero digits
+  const unsigned counters = passes * windows * SORT_RADIX;
+  uint32_t *zero_digits = s_hist + counters;
   const unsigned tile = blockIdx.x;
-  for (unsigned k = threadIdx.x; k < windows * (SORT_RADIX + 1); k += blockDim.x)
-    hist[k] = 0;
+  for (unsigned k = threadIdx.x; k < counters + windows; k += blockDim.x)
+    s_hist[k] = 0;
   __syncthreads();
   const size_t stride = window_stride(n);
+  const unsigned pass_stride = windows * SORT_RADIX;
   auto tile_digits = [&](auto width) {
     constexpr unsigned C = decltype(width)::value;
     // the next scalar is loaded before this one is decomposed, so that its
@@ -49,7 +55,13 @@ __global__ void __launch_bounds__(SORT_THREADS) digits_histogram_kernel(const fe
           const uint32_t key = digit_key(magnitude);
           keys[out] = key;
           vals[out] = i | (negative << 31);
-          atomicAdd(magnitude ? &hist[w * SORT_RADIX + (key & (SORT_RADIX - 1))] : &zero_digits[w], 1u);
+          if (!magnitude) {
+            atomicAdd(&zero_digits[w], 1u);
+            return;
+          }
+          uint32_t *h = s_hist + w * SORT_RADIX;
+          for (unsigned p = 0; p < passes; p++, h += pass_stride)
+            atomicAdd(&h[(key >> (p * SORT_RADIX_BITS)) & (SORT_RADIX - 1)], 1u);
         });
     }
   };
@@ -62,15 +74,44 @@ __global__ void __launch_bounds__(SORT_THREADS) digits_histogram_kernel(const fe
   default: tile_digits(width_constant<0>{}); break;
   }
   __syncthreads();
-  for (unsigned k = threadIdx.x; k < windows * SORT_RADIX; k += blockDim.x)
-    counts[(size_t)k * tiles + tile] = hist[k]; // k = w * 256 + d
+  for (unsigned k = threadIdx.x; k < counters; k += blockDim.x)
+    hist[(size_t)k * tiles + tile] = s_hist[k]; // k = (p * windows + w) * 256 + d
   for (unsigned w = threadIdx.x; w < windows; w += blockDim.x)
     if (zero_digits[w])
       atomicAdd(&zeros[w], zero_digits[w]);
 }
 
+// Stable radix pass (8 bits at `shift`) of every window segment's nonzero
+// entries [w S + zeros[w], w S + n) in one kernel, positions by decoupled
+// look-back (lookback_tile).  Blocks take their tiles in launch order from
+// *tile_ctr (0 at launch), so every tile a block waits for belongs to a block
+// that is already running; consecutive tickets go to different windows
+// (ticket = tile * windows + w), so the tiles in flight spread over all
+// windows and each window's look-back stays short.  Per window: flags[tiles],
+// agg and incl [tiles][256], totals[256].
+__global__ void __launch_bounds__(SORT_THREADS, SORT_SCATTER_MIN_BLOCKS)
+    lookback_stable_kernel(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in, uint32_t *__restrict__ keys_out,
+                           uint32_t *__restrict__ vals_out, unsigned n, unsigned windows, unsigned tiles, unsigned shift, uint32_t *flags,
+                           uint32_t *agg, uint32_t *incl, const uint32_t *__restrict__ totals, const uint32_t *__restrict__ zeros,
+                           unsigned *tile_ctr, unsigned *error) {
+  __shared__ unsigned s_ticket;
+  if (threadIdx.x == 0)
+    s_ticket = atomicAdd(tile_ctr, 1u);
+  __syncthreads();
+  const unsigned w = s_ticket % windows, tile = s_ticket / windows;
+  const unsigned skip = zeros[w], live = n - skip;
+  const unsigned base = tile * SORT_TILE;
+  if (base >= live) // no later tile of this window holds entries either, so none waits for this one
+    return;
+  const size_t rows = (size_t)w * tiles * SORT_RADIX;
+  lookback_tile(keys_in, vals_in, keys_out, vals_out, w * window_stride(n) + skip, tile, min(SORT_TILE, live - base), shift,
+                flags + (size_t)w * tiles, agg + rows, incl + rows, totals + (size_t)w * SORT_RADIX, error);
+}
+
 // ---------------------------------------------------------------------------
-// 2. LSD radix sort, one 8-bit digit per pass, independent per window segment.
+// 2'. LSD radix sort with a histogram and a scan kernel per pass (window
+//    counts above the digit kernel's shared-memory histograms, c <= 5),
+//    one 8-bit digit per pass, independent per window segment.
 //    counts layout: [window][digit][tile]; after sort_scan_kernel it holds,
 //    per (window, digit), the exclusive prefix over tiles, and digit_base
 //    [window][digit] the exclusive prefix over digits: an element's output
@@ -101,12 +142,15 @@ __global__ void __launch_bounds__(SORT_THREADS) sort_histogram_kernel(const uint
   sort_histogram_window<false>(keys, n, tiles, shift, counts, const_cast<uint32_t *>(zeros));
 }
 
-// One warp per (window, digit) row of counts (see sort_scan_row).
-__global__ void __launch_bounds__(256) sort_scan_kernel(uint32_t *counts, unsigned tiles, unsigned rows, uint32_t *__restrict__ totals) {
+// One warp per row of counts (see sort_scan_row): the first prefix_rows rows
+// (pass 0's (window, digit) rows) become exclusive prefixes over the tiles;
+// every row's sum goes to totals[row].
+__global__ void __launch_bounds__(256) sort_scan_kernel(uint32_t *counts, unsigned tiles, unsigned rows, uint32_t *__restrict__ totals,
+                                                        unsigned prefix_rows) {
   const unsigned row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (row >= rows)
     return;
-  sort_scan_row(counts + (size_t)row * tiles, tiles, totals + row);
+  sort_scan_row(counts + (size_t)row * tiles, tiles, totals + row, row < prefix_rows);
 }
 
 __global__ void __launch_bounds__(SORT_THREADS, SORT_SCATTER_MIN_BLOCKS) sort_scatter_first_kernel(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,

@@ -82,6 +82,7 @@ struct plan {
   unsigned log_m;       // log2 of the running-sum group
   unsigned groups;      // G = B / m groups per window
   unsigned log_g;       // gamma = log2 G
+  unsigned sms;         // SMs of the device the plan is for
 };
 
 // ---------------------------------------------------------------------------
@@ -93,11 +94,17 @@ struct plan {
 // and the top window of a W*c >= 254 split never carries out.
 __global__ void digits_kernel(const fe *__restrict__ scalars, unsigned n, unsigned c, unsigned windows, uint32_t *__restrict__ keys,
                               uint32_t *__restrict__ vals);
-// the same, also writing the first radix pass's tile histograms of the
-// nonzero keys and adding each window's zero digits to zeros[w]
-__global__ void digits_histogram_kernel(const fe *__restrict__ scalars, unsigned n, unsigned c, unsigned windows, unsigned tiles,
-                                        uint32_t *__restrict__ keys, uint32_t *__restrict__ vals, uint32_t *__restrict__ counts,
+// the same, one block per sort tile, also counting the tile's nonzero keys
+// per window and radix digit for every sort pass and adding each window's
+// zero digits to zeros[w]
+__global__ void digits_histogram_kernel(const fe *__restrict__ scalars, unsigned n, unsigned c, unsigned windows, unsigned passes, unsigned tiles,
+                                        uint32_t *__restrict__ keys, uint32_t *__restrict__ vals, uint32_t *__restrict__ hist,
                                         uint32_t *__restrict__ zeros);
+// a stable radix pass in one kernel, positions by decoupled look-back
+__global__ void lookback_stable_kernel(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in, uint32_t *__restrict__ keys_out,
+                                       uint32_t *__restrict__ vals_out, unsigned n, unsigned windows, unsigned tiles, unsigned shift, uint32_t *flags,
+                                       uint32_t *agg, uint32_t *incl, const uint32_t *__restrict__ totals, const uint32_t *__restrict__ zeros,
+                                       unsigned *tile_ctr, unsigned *error);
 
 // ---------------------------------------------------------------------------
 // 2. sort (keys and values per window segment of n entries); the first pass
@@ -107,7 +114,7 @@ __global__ void sort_histogram_first_kernel(const uint32_t *__restrict__ keys, u
                                             uint32_t *__restrict__ counts, uint32_t *__restrict__ zeros);
 __global__ void sort_histogram_kernel(const uint32_t *__restrict__ keys, unsigned n, unsigned tiles, unsigned shift, uint32_t *__restrict__ counts,
                                       const uint32_t *__restrict__ zeros);
-__global__ void sort_scan_kernel(uint32_t *counts, unsigned tiles, unsigned rows, uint32_t *__restrict__ totals);
+__global__ void sort_scan_kernel(uint32_t *counts, unsigned tiles, unsigned rows, uint32_t *__restrict__ totals, unsigned prefix_rows);
 // first pass (any order among equal digits) and later passes (stable)
 __global__ void sort_scatter_first_kernel(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in, uint32_t *__restrict__ keys_out,
                                           uint32_t *__restrict__ vals_out, unsigned n, unsigned tiles, unsigned shift,

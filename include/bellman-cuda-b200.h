@@ -37,6 +37,7 @@ typedef struct msm_b200_profile {
   unsigned long long nonempty_buckets; /* buckets that received at least one point */
   unsigned long long heads;            /* accumulation ranges that began inside a bucket */
   unsigned window_bits, windows, acc_threads /* accumulation ranges */, launches;
+  unsigned sort_wait_timeouts; /* radix-pass look-back waits that gave up (0 in correct operation) */
 } msm_b200_profile;
 
 /* Same as msm_b200_execute_async, but synchronises the stream before it

@@ -1,0 +1,143 @@
+"""Integer model of the plain pipeline's radix sort (era-bellman-cuda_b200/csrc/
+msm_kernels.cu: digits_histogram_kernel, sort_scan_kernel,
+sort_scatter_first_kernel, lookback_stable_kernel; tile code in
+msm_device.cuh): per-pass digit counts per tile from the digit kernel, one
+scan giving the first pass's tile offsets and every pass's digit totals, the
+first pass (drops zero digits, any order among equal digits), then one kernel
+per later 8-bit pass in which each tile finds the positions of its digit runs
+by decoupled look-back: it publishes its aggregate, reads the flags of
+earlier tiles 32 at a time until it meets an inclusive count (waiting while a
+tile between has published nothing), adds that count and the aggregates after
+it, and publishes its inclusive count.  Tickets go to windows in turn and
+tiles finish in a random order.  Checked: the window segments come out
+grouped exactly by key (a stable sort of the first pass's output), at
+[w S + zeros_w, w S + n)."""
+import random
+
+import pytest
+
+RADIX_BITS, RADIX, TILE = 8, 256, 64  # the model's tile is small so that windows span many tiles
+AGG, INCL = 1, 2
+ZERO_KEY = 0xFFFFFFFF
+
+
+def digit(key, shift):
+    return (key >> shift) & (RADIX - 1)
+
+
+def model_sort(keys, vals, n, windows, stride, passes, rng):
+    tiles = (n + TILE - 1) // TILE
+    # digit kernel: per (pass, window, tile) counts of the nonzero keys; zeros per window
+    zeros = [0] * windows
+    hist = [[[[0] * RADIX for _ in range(tiles)] for _ in range(windows)] for _ in range(passes)]
+    for w in range(windows):
+        for i in range(n):
+            k = keys[w * stride + i]
+            if k == ZERO_KEY:
+                zeros[w] += 1
+                continue
+            for p in range(passes):
+                hist[p][w][i // TILE][digit(k, p * RADIX_BITS)] += 1
+    # totals kernel; pass 0's counts are published aggregates, later passes' are cleared
+    totals = [[[sum(hist[p][w][t][d] for t in range(tiles)) for d in range(RADIX)] for w in range(windows)] for p in range(passes)]
+    # the scan: pass 0's exclusive prefix over tiles; later passes use look-back
+    scan0 = [[[sum(hist[0][w][u][d] for u in range(t)) for d in range(RADIX)] for t in range(tiles)] for w in range(windows)]
+    flags = [[[0] * tiles for _ in range(windows)] for _ in range(passes)]
+    agg = [[[0] * RADIX for _ in range(tiles)] for _ in range(windows)]
+    incl = [[[0] * RADIX for _ in range(tiles)] for _ in range(windows)]
+    cur_k, cur_v = list(keys), list(vals)
+    for p in range(passes):
+        shift = p * RADIX_BITS
+        out_k, out_v = [None] * len(keys), [None] * len(vals)
+        # every (window, tile) is one block; tickets go to windows in turn
+        # (ticket = tile * windows + w) and blocks progress in a random order;
+        # a block's look-back only ever waits for earlier tiles of its window
+        pending = [(w, t) for t in range(tiles) for w in range(windows)]
+        rng.shuffle(pending)
+        published = set()
+        while pending:
+            progressed = False
+            for item in list(pending):
+                w, t = item
+                live = n if p == 0 else n - zeros[w]
+                base = t * TILE
+                if base >= live:
+                    pending.remove(item)
+                    progressed = True
+                    continue
+                seg_in = w * stride if p == 0 else w * stride + zeros[w]
+                seg_out = w * stride + zeros[w]
+                items = [(cur_k[seg_in + base + i], cur_v[seg_in + base + i]) for i in range(min(TILE, live - base))]
+                if p == 0:
+                    items = [it for it in items if it[0] != ZERO_KEY]
+                    rng.shuffle(items)  # the first pass ranks equal digits in any order
+                count = [0] * RADIX
+                for k, _ in items:
+                    count[digit(k, shift)] += 1
+                if p == 0:
+                    prefix = scan0[w][t]
+                else:
+                    if item not in published:
+                        agg[w][t] = list(count)
+                        flags[p][w][t] = AGG
+                        published.add(item)
+                    # the first warp: flags of 32 earlier tiles at a time
+                    hi, start, blocked = t, -1, False
+                    while hi > 0:
+                        batch = [flags[p][w][hi - 1 - lane] if hi - 1 - lane >= 0 else AGG for lane in range(32)]
+                        nearest = next((lane for lane in range(32) if batch[lane] == INCL), 32)
+                        if any(batch[lane] == 0 for lane in range(nearest)):
+                            blocked = True
+                            break
+                        if nearest < 32:
+                            start = hi - 1 - nearest
+                            break
+                        hi -= 32
+                    if blocked:
+                        continue  # retry later, like the bounded poll
+                    prefix = [(incl[w][start][d] if start >= 0 else 0) + sum(agg[w][j][d] for j in range(start + 1, t)) for d in range(RADIX)]
+                    incl[w][t] = [prefix[d] + count[d] for d in range(RADIX)]
+                    flags[p][w][t] = INCL
+                dbase = [0] * RADIX
+                for d in range(1, RADIX):
+                    dbase[d] = dbase[d - 1] + totals[p][w][d - 1]
+                rank = [0] * RADIX
+                for k, v in items:
+                    d = digit(k, shift)
+                    pos = seg_out + dbase[d] + prefix[d] + rank[d]
+                    rank[d] += 1
+                    assert out_k[pos] is None
+                    out_k[pos], out_v[pos] = k, v
+                pending.remove(item)
+                progressed = True
+            assert progressed, "look-back deadlock"
+        cur_k, cur_v = out_k, out_v
+    return cur_k, cur_v, zeros
+
+
+@pytest.mark.parametrize("trial", range(6))
+def test_onesweep_model_sorts_each_window(trial):
+    rng = random.Random(1000 + trial)
+    key_bits = rng.choice([7, 8, 12, 16])
+    passes = (key_bits + RADIX_BITS - 1) // RADIX_BITS
+    windows = rng.randint(1, 4)
+    n = rng.randint(1, 700)
+    stride = (n + 31) // 32 * 32
+    keys, vals = [ZERO_KEY] * (windows * stride), [0] * (windows * stride)
+    zero_share = rng.choice([0.0, 0.3, 0.9, 1.0])
+    for w in range(windows):
+        hot = rng.randrange(1 << key_bits)
+        for i in range(n):
+            r = rng.random()
+            k = ZERO_KEY if r < zero_share else (hot if r < zero_share + 0.2 else rng.randrange(1 << key_bits))
+            keys[w * stride + i] = k
+            vals[w * stride + i] = i | (rng.randrange(2) << 31)
+    out_k, out_v, zeros = model_sort(keys, vals, n, windows, stride, passes, rng)
+    for w in range(windows):
+        nonzero = [(keys[w * stride + i], vals[w * stride + i]) for i in range(n) if keys[w * stride + i] != ZERO_KEY]
+        assert zeros[w] == n - len(nonzero)
+        got = list(zip(out_k[w * stride + zeros[w]: w * stride + n], out_v[w * stride + zeros[w]: w * stride + n]))
+        # grouped exactly by key; after a stable later pass, the order of
+        # equal full keys is whatever the first pass left (any order)
+        assert [k for k, _ in got] == sorted(k for k, _ in nonzero)
+        assert sorted(got) == sorted(nonzero)
