@@ -192,7 +192,7 @@ __device__ __forceinline__ void sort_histogram_tile(const uint32_t *__restrict__
 // lane (coalesced: each load and store is one 128-byte line), scanned across
 // the warp with shuffles and offset by the running total.  (Lane-contiguous
 // chunks made every load touch 32 lines; at 2^22 the scan kernel took 57 us.)
-__device__ __forceinline__ void sort_scan_row(uint32_t *r, unsigned len, uint32_t *__restrict__ total, bool write_prefix = true) {
+__device__ __forceinline__ void sort_scan_row(uint32_t *r, unsigned len, uint32_t *__restrict__ total) {
   const unsigned lane = threadIdx.x & 31;
   uint32_t run = 0;
   for (unsigned base = 0; base < len; base += 32) {
@@ -205,7 +205,7 @@ __device__ __forceinline__ void sort_scan_row(uint32_t *r, unsigned len, uint32_
       if (lane >= (unsigned)off)
         incl += u;
     }
-    if (t < len && write_prefix)
+    if (t < len)
       r[t] = run + incl - v;
     run += __shfl_sync(0xffffffffu, incl, 31);
   }
@@ -267,11 +267,15 @@ __device__ __forceinline__ void scan_256(const uint32_t *in, uint32_t *out, uint
 // RUN_BASES fills glob[d] (d < SORT_RADIX), the position of this tile's run
 // of digit d relative to seg_out, from the tile's digit counts tile_cnt[]; it
 // is called by every thread of the block (it may synchronise the block) and
-// may use digit_base[] and warp_sums[] as scratch.
-template <bool STABLE, bool DROP_ZEROS, class RUN_BASES>
+// may use digit_base[] and warp_sums[] as scratch.  AFTER() runs on every
+// thread once glob[] is complete, before the tile is staged and written.
+struct no_op {
+  __device__ __forceinline__ void operator()() const {}
+};
+template <bool STABLE, bool DROP_ZEROS, class RUN_BASES, class AFTER = no_op>
 __device__ __forceinline__ void scatter_tile(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in, uint32_t *__restrict__ keys_out,
                                              uint32_t *__restrict__ vals_out, size_t seg_in, size_t seg_out, unsigned base, unsigned count,
-                                             unsigned shift, RUN_BASES run_bases) {
+                                             unsigned shift, RUN_BASES run_bases, AFTER after = AFTER()) {
   __shared__ uint32_t s_key[SORT_TILE];
   __shared__ uint32_t s_val[SORT_TILE];
   __shared__ uint32_t whist[STABLE ? SORT_WARPS : 1][SORT_RADIX];
@@ -329,6 +333,7 @@ __device__ __forceinline__ void scatter_tile(const uint32_t *__restrict__ keys_i
     staged = tile_off[SORT_RADIX - 1] + tile_cnt[SORT_RADIX - 1]; // items kept (dropped zero keys excluded)
   run_bases(static_cast<const uint32_t *>(tile_cnt), glob, digit_base, warp_sums);
   __syncthreads();
+  after();
 #pragma unroll
   for (unsigned r = 0; r < SORT_ITEMS; r++) {
     const unsigned i = sub + r * 32 + lane;
@@ -406,13 +411,18 @@ __device__ __forceinline__ uint32_t load_relaxed(const uint32_t *p) {
 }
 __device__ __forceinline__ void store_release(uint32_t *p, uint32_t v) { asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory"); }
 
-// Publishes this tile's digit counts (all threads call it; one digit per
-// thread) under `flag`.
-__device__ __forceinline__ void lookback_publish(uint32_t *flags, uint32_t *counts, unsigned tile, uint32_t value, uint32_t flag) {
-  counts[(size_t)tile * SORT_RADIX + threadIdx.x] = value;
+// Publishes this tile's digit counts src[0..255] (shared memory) under
+// `flag`: the first warp writes them (eight per lane), makes its writes
+// visible device-wide, then sets the flag.  Called by the first warp only.
+__device__ __forceinline__ void lookback_publish(uint32_t *flags, uint32_t *counts, unsigned tile, const uint32_t *src, uint32_t flag) {
+  const unsigned lane = threadIdx.x & 31;
+  uint32_t *row = counts + (size_t)tile * SORT_RADIX;
+#pragma unroll
+  for (unsigned k = 0; k < SORT_RADIX / 32; k++)
+    row[k * 32 + lane] = src[k * 32 + lane];
   __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0)
+  __syncwarp();
+  if (lane == 0)
     store_release(flags + tile, flag);
 }
 
@@ -430,14 +440,15 @@ __device__ __forceinline__ void lookback_tile(const uint32_t *__restrict__ keys_
                                               uint32_t *__restrict__ keys_out, uint32_t *__restrict__ vals_out, size_t seg, unsigned tile,
                                               unsigned count, unsigned shift, uint32_t *flags, uint32_t *agg, uint32_t *incl,
                                               const uint32_t *__restrict__ totals, unsigned *error) {
+  __shared__ uint32_t s_incl[SORT_RADIX]; // this tile's inclusive counts, published after the bases are known
   scatter_tile<true, false>(
       keys_in, vals_in, keys_out, vals_out, seg, seg, tile * SORT_TILE, count, shift,
       [&](const uint32_t *tile_cnt, uint32_t *glob, uint32_t *digit_base, uint32_t *warp_sums) {
         __shared__ int s_start;
         const unsigned d = threadIdx.x, lane = threadIdx.x & 31;
         const uint32_t own = tile_cnt[d];
-        lookback_publish(flags, agg, tile, own, LOOKBACK_AGGREGATE);
         if (threadIdx.x < 32) {
+          lookback_publish(flags, agg, tile, tile_cnt, LOOKBACK_AGGREGATE);
           int hi = (int)tile; // tiles [0, hi) are still to be examined
           int start = -1;     // nearest earlier tile with an inclusive count
           unsigned polls = 0;
@@ -481,7 +492,11 @@ __device__ __forceinline__ void lookback_tile(const uint32_t *__restrict__ keys_
               prefix += load_relaxed(agg + (size_t)j * SORT_RADIX + d);
         }
         glob[d] = digit_base[d] + prefix;
-        lookback_publish(flags, incl, tile, prefix + own, LOOKBACK_INCLUSIVE);
+        s_incl[d] = prefix + own;
+      },
+      [&] { // the first warp publishes the inclusive counts; the others go on
+        if (threadIdx.x < 32)
+          lookback_publish(flags, incl, tile, s_incl, LOOKBACK_INCLUSIVE);
       });
 }
 

@@ -226,13 +226,13 @@ static layout make_layout(const plan &p, bool copy_scalars, bool copy_bases, boo
     l.keys[i] = take(entries * 4);
     l.vals[i] = take(entries * 4);
   }
-  // digit counts per (pass, window, digit, tile); then one region cleared per
+  // the first pass's digit counts per (window, digit, tile); then one region cleared per
   // chunk: digit totals per (pass, window, digit), zero digits per window, a
   // tile counter per pass, the look-back error word and the look-back flags
   // of the passes after the first; then the look-back counts (shared by those
   // passes)
   const size_t lookback_words = (size_t)p.windows * p.tiles;
-  l.counts = take((size_t)p.sort_passes * p.windows * SORT_RADIX * p.tiles * 4);
+  l.counts = take((size_t)p.windows * SORT_RADIX * p.tiles * 4);
   l.sort_small_bytes = ((size_t)p.sort_passes * p.windows * SORT_RADIX + p.windows + p.sort_passes + 1 + (p.sort_passes - 1) * lookback_words) * 4;
   l.totals = take(l.sort_small_bytes);
   l.zeros = l.totals + (size_t)p.sort_passes * p.windows * SORT_RADIX * 4;
@@ -345,15 +345,15 @@ static cudaError_t enqueue_accumulation(const plan &p, const fe *scalars, const 
   if (p.windows <= MAX_FUSED_HISTOGRAM_WINDOWS) {
     // 1. digits, with every pass's digit counts per tile
     digits_histogram_kernel<<<p.tiles, SORT_THREADS, digit_histogram_smem(p.windows, p.sort_passes), stream>>>(
-        scalars, n, p.c, p.windows, p.sort_passes, p.tiles, keys[0], vals[0], counts, zeros);
+        scalars, n, p.c, p.windows, p.sort_passes, p.tiles, keys[0], vals[0], counts, totals, zeros);
     CHECK(cudaGetLastError());
     m.launched++;
     CHECK(m.mark(stream));
-    // 2. sort: one scan for the first pass's tile offsets and every pass's
-    // digit totals, the first pass (drops zero digits), then one look-back
-    // kernel per later 8-bit pass
-    const unsigned prefix_rows = p.windows * SORT_RADIX, rows = p.sort_passes * prefix_rows;
-    sort_scan_kernel<<<(rows * 32 + 255) / 256, 256, 0, stream>>>(counts, p.tiles, rows, totals, prefix_rows);
+    // 2. sort: one scan for the first pass's tile offsets and digit totals,
+    // the first pass (drops zero digits), then one look-back kernel per later
+    // 8-bit pass (their digit totals come from the digit kernel)
+    const unsigned prefix_rows = p.windows * SORT_RADIX;
+    sort_scan_kernel<<<(prefix_rows * 32 + 255) / 256, 256, 0, stream>>>(counts, p.tiles, prefix_rows, totals);
     CHECK(cudaGetLastError());
     const dim3 grid(p.tiles, p.windows);
     sort_scatter_first_kernel<<<grid, SORT_THREADS, 0, stream>>>(keys[0], vals[0], keys[1], vals[1], n, p.tiles, 0, counts, totals, zeros);
@@ -387,7 +387,7 @@ static cudaError_t enqueue_accumulation(const plan &p, const fe *scalars, const 
       else
         sort_histogram_kernel<<<grid, SORT_THREADS, 0, stream>>>(keys[cur], n, p.tiles, shift, counts, zeros);
       CHECK(cudaGetLastError());
-      sort_scan_kernel<<<(rows * 32 + 255) / 256, 256, 0, stream>>>(counts, p.tiles, rows, totals, rows);
+      sort_scan_kernel<<<(rows * 32 + 255) / 256, 256, 0, stream>>>(counts, p.tiles, rows, totals);
       CHECK(cudaGetLastError());
       if (pass == 0)
         sort_scatter_first_kernel<<<grid, SORT_THREADS, 0, stream>>>(keys[cur], vals[cur], keys[cur ^ 1], vals[cur ^ 1], n, p.tiles, shift, counts,

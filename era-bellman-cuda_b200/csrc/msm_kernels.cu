@@ -19,14 +19,15 @@ __global__ void __launch_bounds__(256) digits_kernel(const fe *__restrict__ scal
 // The same, one block per sort tile (SORT_TILE scalars), also counting the
 // tile's nonzero keys per window and radix digit for every sort pass
 // (dynamic shared memory: passes x windows x 256 counters, then windows zero
-// counters): hist[((p * windows + w) * 256 + d) * tiles + tile] receives the
-// count of digit d of pass p.  sort_scan_kernel turns pass 0's counts into
-// the first radix pass's tile offsets and every pass's into digit totals.
-// Each window's zero digits are added to zeros[w].
+// counters).  Pass 0's counts go to hist[(w * 256 + d) * tiles + tile], which
+// sort_scan_kernel turns into the first radix pass's tile offsets and digit
+// totals; later passes need only their digit totals, which the block adds to
+// totals[(p * windows + w) * 256 + d] (zero at launch).  Each window's zero
+// digits are added to zeros[w].
 __global__ void __launch_bounds__(SORT_THREADS) digits_histogram_kernel(const fe *__restrict__ scalars, unsigned n, unsigned c, unsigned windows,
                                                                         unsigned passes, unsigned tiles, uint32_t *__restrict__ keys,
                                                                         uint32_t *__restrict__ vals, uint32_t *__restrict__ hist,
-                                                                        uint32_t *__restrict__ zeros) {
+                                                                        uint32_t *__restrict__ totals, uint32_t *__restrict__ zeros) {
   extern __shared__ uint32_t s_hist[]; // [passes][windows][SORT_RADIX], then [windows] zero digits
   const unsigned counters = passes * windows * SORT_RADIX;
   uint32_t *zero_digits = s_hist + counters;
@@ -74,8 +75,11 @@ __global__ void __launch_bounds__(SORT_THREADS) digits_histogram_kernel(const fe
   default: tile_digits(width_constant<0>{}); break;
   }
   __syncthreads();
-  for (unsigned k = threadIdx.x; k < counters; k += blockDim.x)
-    hist[(size_t)k * tiles + tile] = s_hist[k]; // k = (p * windows + w) * 256 + d
+  for (unsigned k = threadIdx.x; k < pass_stride; k += blockDim.x)
+    hist[(size_t)k * tiles + tile] = s_hist[k]; // k = w * 256 + d
+  for (unsigned k = pass_stride + threadIdx.x; k < counters; k += blockDim.x)
+    if (s_hist[k])
+      atomicAdd(&totals[k], s_hist[k]); // k = (p * windows + w) * 256 + d
   for (unsigned w = threadIdx.x; w < windows; w += blockDim.x)
     if (zero_digits[w])
       atomicAdd(&zeros[w], zero_digits[w]);
@@ -142,15 +146,12 @@ __global__ void __launch_bounds__(SORT_THREADS) sort_histogram_kernel(const uint
   sort_histogram_window<false>(keys, n, tiles, shift, counts, const_cast<uint32_t *>(zeros));
 }
 
-// One warp per row of counts (see sort_scan_row): the first prefix_rows rows
-// (pass 0's (window, digit) rows) become exclusive prefixes over the tiles;
-// every row's sum goes to totals[row].
-__global__ void __launch_bounds__(256) sort_scan_kernel(uint32_t *counts, unsigned tiles, unsigned rows, uint32_t *__restrict__ totals,
-                                                        unsigned prefix_rows) {
+// One warp per (window, digit) row of counts (see sort_scan_row).
+__global__ void __launch_bounds__(256) sort_scan_kernel(uint32_t *counts, unsigned tiles, unsigned rows, uint32_t *__restrict__ totals) {
   const unsigned row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (row >= rows)
     return;
-  sort_scan_row(counts + (size_t)row * tiles, tiles, totals + row, row < prefix_rows);
+  sort_scan_row(counts + (size_t)row * tiles, tiles, totals + row);
 }
 
 __global__ void __launch_bounds__(SORT_THREADS, SORT_SCATTER_MIN_BLOCKS) sort_scatter_first_kernel(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,

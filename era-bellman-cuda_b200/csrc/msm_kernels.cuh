@@ -99,7 +99,7 @@ __global__ void digits_kernel(const fe *__restrict__ scalars, unsigned n, unsign
 // zero digits to zeros[w]
 __global__ void digits_histogram_kernel(const fe *__restrict__ scalars, unsigned n, unsigned c, unsigned windows, unsigned passes, unsigned tiles,
                                         uint32_t *__restrict__ keys, uint32_t *__restrict__ vals, uint32_t *__restrict__ hist,
-                                        uint32_t *__restrict__ zeros);
+                                        uint32_t *__restrict__ totals, uint32_t *__restrict__ zeros);
 // a stable radix pass in one kernel, positions by decoupled look-back
 __global__ void lookback_stable_kernel(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in, uint32_t *__restrict__ keys_out,
                                        uint32_t *__restrict__ vals_out, unsigned n, unsigned windows, unsigned tiles, unsigned shift, uint32_t *flags,
@@ -114,7 +114,7 @@ __global__ void sort_histogram_first_kernel(const uint32_t *__restrict__ keys, u
                                             uint32_t *__restrict__ counts, uint32_t *__restrict__ zeros);
 __global__ void sort_histogram_kernel(const uint32_t *__restrict__ keys, unsigned n, unsigned tiles, unsigned shift, uint32_t *__restrict__ counts,
                                       const uint32_t *__restrict__ zeros);
-__global__ void sort_scan_kernel(uint32_t *counts, unsigned tiles, unsigned rows, uint32_t *__restrict__ totals, unsigned prefix_rows);
+__global__ void sort_scan_kernel(uint32_t *counts, unsigned tiles, unsigned rows, uint32_t *__restrict__ totals);
 // first pass (any order among equal digits) and later passes (stable)
 __global__ void sort_scatter_first_kernel(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in, uint32_t *__restrict__ keys_out,
                                           uint32_t *__restrict__ vals_out, unsigned n, unsigned tiles, unsigned shift,

@@ -1,9 +1,10 @@
 """Integer model of the plain pipeline's radix sort (era-bellman-cuda_b200/csrc/
 msm_kernels.cu: digits_histogram_kernel, sort_scan_kernel,
 sort_scatter_first_kernel, lookback_stable_kernel; tile code in
-msm_device.cuh): per-pass digit counts per tile from the digit kernel, one
-scan giving the first pass's tile offsets and every pass's digit totals, the
-first pass (drops zero digits, any order among equal digits), then one kernel
+msm_device.cuh): per-pass digit counts per tile from the digit kernel (the
+first pass's per tile, later passes' summed into digit totals), one scan
+giving the first pass's tile offsets and totals, the first pass (drops zero
+digits, any order among equal digits), then one kernel
 per later 8-bit pass in which each tile finds the positions of its digit runs
 by decoupled look-back: it publishes its aggregate, reads the flags of
 earlier tiles 32 at a time until it meets an inclusive count (waiting while a
