@@ -217,7 +217,16 @@ bc_error msm_b200_execute_no_alloc_async(bc_stream stream, const void *bases, co
  * reads and writes it in place); a null or pageable pointer, or another
  * device's memory without that peer access, returns bc_error_invalid_value
  * before anything is enqueued.  Asynchronous on `stream`, one kernel of one block, no
- * allocation.  Enqueue it after the MSM on the same stream. */
+ * allocation.  Enqueue it after the MSM on the same stream.
+ *
+ * Speed: this is not a faster Horner pass.  The sum needs 253 doublings in a
+ * dependent chain whatever the order, and one GPU thread's carry chains are
+ * slower than a host core's 64-bit products: about 0.58 ms per call on a B200
+ * for this library's plain results, against about 0.21 ms for the Horner
+ * pass on one host core of the same machine (0.13 ms here for batched
+ * results, whose upper bits are infinity).  Use it when the point is wanted
+ * on the device, or when the host should do no work; otherwise the host pass
+ * is quicker. */
 typedef struct msm_b200_affine_point {
   uint32_t x[8];
   uint32_t y[8];
