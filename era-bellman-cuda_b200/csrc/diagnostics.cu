@@ -110,8 +110,10 @@ __global__ void __launch_bounds__(128) montmul_kernel(uint32_t seed, unsigned it
   sink[tid] = x.l[0] ^ z.l[1];
 }
 
-// kind 3: XYZZ += affine chain (never the doubling branch: acc = k*G, k >= 2)
-__global__ void __launch_bounds__(128) madd_kernel(unsigned iters, uint32_t *sink) {
+// kind 3: XYZZ += affine chain with add_affine_finite, the addition of the
+// accumulation loop (never the doubling or cancelling branch: acc = k*G,
+// k >= 2), at the accumulation kernel's 4 blocks of 128 threads per SM
+__global__ void __launch_bounds__(128, 4) madd_kernel(unsigned iters, uint32_t *sink) {
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
   fe one_std = fq::zero(), two_std = fq::zero();
   one_std.l[0] = 1;
@@ -122,9 +124,10 @@ __global__ void __launch_bounds__(128) madd_kernel(unsigned iters, uint32_t *sin
   if (tid & 1)
     g.y = fq::neg(g.y);
   xyzz acc = curve::dbl_affine(g);
+  bool inf = false;
   for (unsigned i = 0; i < iters; i++)
-    acc = curve::add_affine(acc, g);
-  sink[tid] = acc.x.l[0] ^ acc.zz.l[3];
+    acc = curve::add_affine_finite(acc, g, inf);
+  sink[tid] = acc.x.l[0] ^ acc.zz.l[3] ^ (inf ? 1u : 0u);
 }
 
 } // namespace
