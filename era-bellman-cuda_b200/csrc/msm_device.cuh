@@ -293,12 +293,19 @@ __device__ __forceinline__ void scatter_tile(const uint32_t *__restrict__ keys_i
   __syncthreads();
   uint32_t key[SORT_ITEMS], val[SORT_ITEMS], rank[SORT_ITEMS];
   const unsigned lt_mask = (1u << lane) - 1;
+  // every item's loads first, so that all of them are in flight together
+  // (loads interleaved with the ranking rounds wait one round at a time: the
+  // sort stage took 0.917 against 0.836 ms at 2^22), then the ranking
+#pragma unroll
+  for (unsigned r = 0; r < SORT_ITEMS; r++) {
+    const unsigned i = sub + r * 32 + lane;
+    key[r] = i < count ? keys_in[seg_in + base + i] : 0;
+    val[r] = i < count ? vals_in[seg_in + base + i] : 0;
+  }
 #pragma unroll
   for (unsigned r = 0; r < SORT_ITEMS; r++) {
     const unsigned i = sub + r * 32 + lane;
     const bool in_tile = i < count;
-    key[r] = in_tile ? keys_in[seg_in + base + i] : 0;
-    val[r] = in_tile ? vals_in[seg_in + base + i] : 0;
     const bool valid = in_tile && (!DROP_ZEROS || key[r] != ZERO_KEY);
     const unsigned d = valid ? sort_digit(key[r], shift) : SORT_RADIX;
     if (STABLE) {
