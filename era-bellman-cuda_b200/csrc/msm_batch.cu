@@ -9,8 +9,9 @@
 // A batch is a fixed list of instance sizes n_k (any lengths, prefixes of the
 // table).  All instances run as one kernel chain:
 //   digits       every point of every instance, W(c_k) signed digits each, into
-//                its instance's segment of W(c_k) windows of window_stride(n_k)
-//                (key, value) entries (the padding holds zero digits)
+//                its instance's segment of W(c_k) windows of n_k rounded up
+//                to whole sort tiles (the padding holds zero digits), with the
+//                first radix pass's tile counts
 //   sort         segmented LSD radix sort, tile list over all segments; the
 //                first pass drops zero digits (counted per segment)
 //   accumulate   the nonzero entries of all segments split into equal ranges,
@@ -93,69 +94,100 @@ __global__ void __launch_bounds__(128) window_multiples_kernel(const affine *__r
   next[i] = curve::to_affine(p); // 2^(cj) P is never infinity: the group order r is an odd prime
 }
 
-// One thread per point of the batch (instances concatenated).
-__global__ void __launch_bounds__(256) batch_digits_kernel(const batch_instance *__restrict__ inst, const unsigned *__restrict__ point_offset,
-                                                           unsigned instances, unsigned total_points, const batch_io *__restrict__ io,
-                                                           uint32_t *__restrict__ keys, uint32_t *__restrict__ vals) {
-  __shared__ unsigned s_off[MAX_BATCH + 1];
-  for (unsigned k = threadIdx.x; k <= instances; k += blockDim.x)
-    s_off[k] = point_offset[k];
-  __syncthreads();
-  const unsigned g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= total_points)
-    return;
-  unsigned lo = 0, hi = instances; // largest k with s_off[k] <= g
-  while (hi - lo > 1) {
-    const unsigned mid = (lo + hi) >> 1;
-    if (s_off[mid] <= g)
-      lo = mid;
-    else
-      hi = mid;
-  }
-  const unsigned k = lo, i = g - s_off[k];
+// One block per point tile (SORT_TILE consecutive points of one instance;
+// the padding points n <= i < seg_stride hold zero digits): every window's
+// signed digit of each point into the instance's segment (entry w *
+// seg_stride + i, value = table index w * stride + i with the sign), and, in
+// shared memory (windows x 256 counters), the tile's nonzero keys per window
+// and low radix digit.  Since seg_stride is a whole number of sort tiles,
+// the entries of window w of this point tile are exactly sort tile w *
+// point_tiles + p of the segment, so these are the first radix pass's tile
+// counts, written for batch_sort_scan_kernel (no histogram kernel for that
+// pass).  Zero digits (padding included) are added to zeros[k].
+__global__ void __launch_bounds__(SORT_THREADS) batch_digits_histogram_kernel(const batch_instance *__restrict__ inst,
+                                                                              const unsigned *__restrict__ ptile_seg, const batch_io *__restrict__ io,
+                                                                              uint32_t *__restrict__ keys, uint32_t *__restrict__ vals,
+                                                                              uint32_t *__restrict__ counts, uint32_t *__restrict__ zeros) {
+  extern __shared__ uint32_t s_hist[]; // [windows][SORT_RADIX], then the zero-digit count
+  const unsigned k = ptile_seg[blockIdx.x];
   const batch_instance d = inst[k];
+  const unsigned tile = blockIdx.x - d.ptile_base, windows = d.windows;
+  const unsigned counters = windows * SORT_RADIX;
+  uint32_t *zero_digits = s_hist + counters;
+  for (unsigned q = threadIdx.x; q <= counters; q += blockDim.x)
+    s_hist[q] = 0;
+  __syncthreads();
   const fe *scalars = io[k].scalars;
-  const fe scalar = load_fe_streaming(scalars + i);
-  const size_t window_base = d.entry_offset, stride = window_stride(d.n);
-  auto digits = [&](auto width) {
-    scalar_digits_fixed<decltype(width)::value>(scalar, d.c, d.windows, [&](unsigned w, uint32_t magnitude, uint32_t negative) {
-      const size_t out = window_base + w * stride + i;
-      keys[out] = digit_key(magnitude);
-      vals[out] = (w * d.stride + i) | (negative << 31);
-    });
-  };
-  // the padding after each window (its segment is window_stride(n) long)
-  // holds zero digits, which the first sort pass drops; point i fills padding
-  // slots i, i + n, ... (an instance may have fewer points than padding slots)
-  for (size_t j = i; j < stride - d.n; j += d.n)
-    for (unsigned w = 0; w < d.windows; w++) {
-      keys[window_base + w * stride + d.n + j] = ZERO_KEY;
-      vals[window_base + w * stride + d.n + j] = 0;
+  const size_t S = d.seg_stride;
+  const unsigned first = tile * SORT_TILE + threadIdx.x;
+  uint32_t zero_count = 0;
+  auto tile_digits = [&](auto width) {
+    constexpr unsigned C = decltype(width)::value;
+    // the next scalar is loaded before this one is decomposed
+    fe next = fr::zero();
+    if (first < d.n)
+      next = load_fe_streaming(scalars + first);
+    for (unsigned q = 0; q < SORT_ITEMS; q++) {
+      const unsigned i = first + q * SORT_THREADS; // < seg_stride
+      const fe scalar = next;
+      if (q + 1 < SORT_ITEMS && i + SORT_THREADS < d.n)
+        next = load_fe_streaming(scalars + i + SORT_THREADS);
+      if (i < d.n) {
+        scalar_digits_fixed<C>(scalar, d.c, windows, [&](unsigned w, uint32_t magnitude, uint32_t negative) {
+          const size_t out = d.entry_offset + w * S + i;
+          const uint32_t key = digit_key(magnitude);
+          keys[out] = key;
+          vals[out] = (w * d.stride + i) | (negative << 31);
+          if (magnitude)
+            atomicAdd(&s_hist[w * SORT_RADIX + (key & (SORT_RADIX - 1))], 1u);
+          else
+            zero_count++;
+        });
+      } else {
+        for (unsigned w = 0; w < windows; w++) {
+          keys[d.entry_offset + w * S + i] = ZERO_KEY;
+          vals[d.entry_offset + w * S + i] = 0;
+        }
+        zero_count += windows;
+      }
     }
+  };
   // the widths the batch table picks for its large instances get unrolled code
   switch (d.c) {
-  case 16: digits(width_constant<16>{}); break;
-  case 17: digits(width_constant<17>{}); break;
-  case 20: digits(width_constant<20>{}); break;
-  case 22: digits(width_constant<22>{}); break;
-  default: digits(width_constant<0>{}); break;
+  case 16: tile_digits(width_constant<16>{}); break;
+  case 17: tile_digits(width_constant<17>{}); break;
+  case 20: tile_digits(width_constant<20>{}); break;
+  case 22: tile_digits(width_constant<22>{}); break;
+  default: tile_digits(width_constant<0>{}); break;
   }
+  if (zero_count)
+    atomicAdd(zero_digits, zero_count);
+  __syncthreads();
+  for (unsigned q = threadIdx.x; q < counters; q += blockDim.x) { // q = w * 256 + digit
+    const unsigned w = q / SORT_RADIX, dg = q % SORT_RADIX;
+    counts[(size_t)d.tile_base * SORT_RADIX + (size_t)dg * d.tiles + w * d.point_tiles + tile] = s_hist[q];
+  }
+  if (threadIdx.x == 0 && *zero_digits)
+    atomicAdd(&zeros[k], *zero_digits);
 }
 
-// The first pass drops zero digits (counted into zeros[k], which must start at
-// 0) and writes the nonzero entries of instance k to the end of its segment;
-// later passes sort that range only.
-template <bool FIRST>
+// Dynamic shared memory of batch_digits_histogram_kernel for an instance of
+// window width c: a counter per (window, digit) and the zero-digit count.
+static size_t batch_digit_smem(unsigned c) { return ((size_t)windows_for(c) * SORT_RADIX + 1) * 4; }
+
+// A later radix pass's tile counts of every segment's nonzero entries
+// [entry_offset + zeros[k], entry_offset + entries), where the first pass
+// put them.
 __global__ void __launch_bounds__(SORT_THREADS) batch_sort_histogram_kernel(const uint32_t *__restrict__ keys, const batch_instance *__restrict__ inst,
                                                                             const unsigned *__restrict__ tile_seg, unsigned shift,
-                                                                            uint32_t *__restrict__ counts, uint32_t *__restrict__ zeros) {
+                                                                            uint32_t *__restrict__ counts, const uint32_t *__restrict__ zeros) {
   const unsigned t = blockIdx.x;
   const unsigned k = tile_seg[t];
   const batch_instance d = inst[k];
-  const unsigned skip = FIRST ? 0 : zeros[k], live = d.entries - skip;
+  const unsigned skip = zeros[k], live = d.entries - skip;
   const unsigned local = t - d.tile_base, base = local * SORT_TILE;
-  sort_histogram_tile<FIRST>(keys + d.entry_offset + skip, base, base < live ? min(SORT_TILE, live - base) : 0, shift,
-                             counts + (size_t)d.tile_base * SORT_RADIX + local, d.tiles, zeros + k);
+  sort_histogram_tile<false>(keys + d.entry_offset + skip, base, base < live ? min(SORT_TILE, live - base) : 0, shift,
+                             counts + (size_t)d.tile_base * SORT_RADIX + local, d.tiles, nullptr);
 }
 
 // one warp per (segment, digit) row
@@ -434,7 +466,6 @@ cudaError_t make_batch_plan(batch_plan &b, const base_table_impl *table, const u
   b = batch_plan{};
   b.instances = instances;
   b.inst.resize(instances);
-  b.point_offset.assign(instances + 1, 0);
   // instance geometry; reduction groups by window width (buckets of a group contiguous)
   std::map<unsigned, std::vector<unsigned>> by_c;
   unsigned max_c = 0;
@@ -450,22 +481,28 @@ cudaError_t make_batch_plan(batch_plan &b, const base_table_impl *table, const u
     d.windows = windows_for(c);
     d.stride = table->prefix[c];
     d.table = table->mult[c];
-    if ((unsigned long long)d.windows * window_stride(n) >= (1ull << 31) || d.windows * (unsigned long long)d.stride >= (1ull << 31))
+    const unsigned long long seg_stride = ((unsigned long long)n + SORT_TILE - 1) / SORT_TILE * SORT_TILE;
+    if (d.windows * seg_stride >= (1ull << 31) || d.windows * (unsigned long long)d.stride >= (1ull << 31))
       return cudaErrorInvalidValue;
-    d.entries = d.windows * (unsigned)window_stride(n); // windows start on 128-byte lines (window_stride)
+    // every window of the segment is a whole number of sort tiles, so the
+    // digit kernel's point tiles count exactly the first pass's sort tiles
+    d.seg_stride = (unsigned)seg_stride;
+    d.point_tiles = d.seg_stride / SORT_TILE;
+    d.entries = d.windows * d.seg_stride;
     d.entry_offset = b.total_entries;
-    d.tiles = (d.entries + SORT_TILE - 1) / SORT_TILE;
+    d.tiles = d.windows * d.point_tiles;
     d.tile_base = b.total_tiles;
+    d.ptile_base = b.total_point_tiles;
     b.total_entries += d.entries;
     b.total_tiles += d.tiles;
-    b.point_offset[k] = (unsigned)points;
+    b.total_point_tiles += d.point_tiles;
+    b.digit_smem = std::max(b.digit_smem, batch_digit_smem(c));
     points += n;
     max_c = std::max(max_c, c);
     by_c[c].push_back(k);
   }
   if (points >= (1ull << 32) || b.total_tiles >= (1u << 31))
     return cudaErrorInvalidValue;
-  b.point_offset[instances] = (unsigned)points;
   b.total_points = (unsigned)points;
   b.sort_passes = (max_c - 1 + SORT_RADIX_BITS - 1) / SORT_RADIX_BITS; // keys take c - 1 bits
   for (auto &kv : by_c) {
@@ -513,8 +550,8 @@ cudaError_t make_batch_plan(batch_plan &b, const base_table_impl *table, const u
   // constant descriptors last, in one contiguous range (one upload)
   b.descriptors = off;
   b.inst_dev = take(instances * sizeof(batch_instance));
-  b.point_offset_dev = take((instances + 1) * 4);
   b.tile_seg_dev = take((size_t)b.total_tiles * 4);
+  b.ptile_seg_dev = take((size_t)b.total_point_tiles * 4);
   for (batch_group &g : b.groups)
     g.members_dev = take(g.members.size() * 4);
   b.bytes = off;
@@ -526,10 +563,12 @@ std::vector<uint8_t> descriptor_image(const batch_plan &b) {
   std::vector<uint8_t> img(b.bytes - b.descriptors, 0);
   auto put = [&](size_t off, const void *src, size_t bytes) { std::memcpy(img.data() + (off - b.descriptors), src, bytes); };
   put(b.inst_dev, b.inst.data(), b.instances * sizeof(batch_instance));
-  put(b.point_offset_dev, b.point_offset.data(), (b.instances + 1) * 4);
   unsigned *tile_seg = reinterpret_cast<unsigned *>(img.data() + (b.tile_seg_dev - b.descriptors));
-  for (unsigned k = 0; k < b.instances; k++)
+  unsigned *ptile_seg = reinterpret_cast<unsigned *>(img.data() + (b.ptile_seg_dev - b.descriptors));
+  for (unsigned k = 0; k < b.instances; k++) {
     std::fill(tile_seg + b.inst[k].tile_base, tile_seg + b.inst[k].tile_base + b.inst[k].tiles, k);
+    std::fill(ptile_seg + b.inst[k].ptile_base, ptile_seg + b.inst[k].ptile_base + b.inst[k].point_tiles, k);
+  }
   for (const batch_group &g : b.groups)
     put(g.members_dev, g.members.data(), g.members.size() * 4);
   return img;
@@ -556,19 +595,20 @@ cudaError_t enqueue_batch(const batch_plan &b, uint8_t *scratch, cudaStream_t s,
 
   CHECK(cudaMemsetAsync(flags, 0, b.slots, s));
   CHECK(cudaMemsetAsync(zeros, 0, b.instances * sizeof(uint32_t), s));
-  batch_digits_kernel<<<(b.total_points + 255) / 256, 256, 0, s>>>(inst, reinterpret_cast<const unsigned *>(at(b.point_offset_dev)), b.instances,
-                                                                   b.total_points, io, keys[0], vals[0]);
+  // digits, with the first pass's counts per sort tile
+  batch_digits_histogram_kernel<<<b.total_point_tiles, SORT_THREADS, b.digit_smem, s>>>(
+      inst, reinterpret_cast<const unsigned *>(at(b.ptile_seg_dev)), io, keys[0], vals[0], counts, zeros);
   CHECK(cudaGetLastError());
   launched++;
   int cur = 0;
   const unsigned rows = b.instances * SORT_RADIX;
   for (unsigned pass = 0; pass < b.sort_passes; pass++) {
     const unsigned shift = pass * SORT_RADIX_BITS;
-    if (pass == 0)
-      batch_sort_histogram_kernel<true><<<b.total_tiles, SORT_THREADS, 0, s>>>(keys[cur], inst, tile_seg, shift, counts, zeros);
-    else
-      batch_sort_histogram_kernel<false><<<b.total_tiles, SORT_THREADS, 0, s>>>(keys[cur], inst, tile_seg, shift, counts, zeros);
-    CHECK(cudaGetLastError());
+    if (pass > 0) {
+      batch_sort_histogram_kernel<<<b.total_tiles, SORT_THREADS, 0, s>>>(keys[cur], inst, tile_seg, shift, counts, zeros);
+      CHECK(cudaGetLastError());
+      launched++;
+    }
     batch_sort_scan_kernel<<<(rows * 32 + 255) / 256, 256, 0, s>>>(counts, inst, rows, totals);
     CHECK(cudaGetLastError());
     if (pass == 0)
@@ -578,7 +618,7 @@ cudaError_t enqueue_batch(const batch_plan &b, uint8_t *scratch, cudaStream_t s,
       batch_sort_scatter_kernel<true><<<b.total_tiles, SORT_THREADS, 0, s>>>(keys[cur], vals[cur], keys[cur ^ 1], vals[cur ^ 1], inst, tile_seg,
                                                                             shift, counts, totals, zeros);
     CHECK(cudaGetLastError());
-    launched += 3;
+    launched += 2;
     cur ^= 1;
   }
   unsigned *work = reinterpret_cast<unsigned *>(at(b.work));
@@ -733,6 +773,10 @@ cudaError_t batch_execute(batch_impl *bi, const void *const *scalars, void *cons
 
 cudaError_t batch_set_up() {
   CHECK(cudaFuncSetAttribute(batch_accumulate_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 50));
+  size_t digit_smem = 0; // the widest instance any batch can hold
+  for (unsigned c = 2; c <= MAX_TABLE_BITS; c++)
+    digit_smem = std::max(digit_smem, batch_digit_smem(c));
+  CHECK(cudaFuncSetAttribute(batch_digits_histogram_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)digit_smem));
   return cudaSuccess;
 }
 

@@ -18,9 +18,12 @@ struct batch_instance {
   unsigned long long entry_offset; // first entry of the instance's segment
   const affine *table;             // M_c: table[j * stride + i] = 2^(c j) P_i
   unsigned n, c, windows, stride;
-  unsigned entries;     // windows * n
-  unsigned tiles;       // sort tiles of the segment
+  unsigned seg_stride;  // entries per window in the segment: n rounded up to whole sort tiles (the padding holds zero digits)
+  unsigned entries;     // windows * seg_stride
+  unsigned tiles;       // sort tiles of the segment (windows * point_tiles)
   unsigned tile_base;   // first global sort tile of the segment
+  unsigned point_tiles; // sort tiles per window: seg_stride / SORT_TILE
+  unsigned ptile_base;  // first global point tile (digit-kernel block) of the instance
   unsigned bucket_base; // first bucket slot (slot 0 holds |d| = 2^(c-1))
 };
 
@@ -57,11 +60,11 @@ struct batch_group {
 struct batch_plan {
   unsigned instances = 0;
   unsigned long long total_entries = 0;
-  unsigned total_points = 0, total_tiles = 0, slots = 0, sort_passes = 0, acc_threads = 0, acc_ranges = 0;
+  unsigned total_points = 0, total_tiles = 0, total_point_tiles = 0, slots = 0, sort_passes = 0, acc_threads = 0, acc_ranges = 0;
   std::vector<batch_instance> inst;
-  std::vector<unsigned> point_offset;
   std::vector<batch_group> groups;
-  size_t keys[2], vals[2], counts, totals, zeros, buckets, flags, hb[2], hp[2], work, inst_dev, point_offset_dev, tile_seg_dev, io;
+  size_t keys[2], vals[2], counts, totals, zeros, buckets, flags, hb[2], hp[2], work, inst_dev, tile_seg_dev, ptile_seg_dev, io;
+  size_t digit_smem = 0; // dynamic shared memory of the digit kernel (its widest instance)
   size_t bytes = 0;       // scratch bytes
   size_t descriptors = 0; // offset of the constant descriptors (inst_dev .. end of members)
 };
