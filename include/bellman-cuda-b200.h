@@ -124,7 +124,7 @@ bc_error msm_b200_batch_create(msm_b200_batch *batch, msm_b200_base_table table,
  * batch share its scratch: serialise them (one stream). */
 bc_error msm_b200_batch_execute_async(msm_b200_batch batch, const void *const *scalars, void *const *results, bc_stream stream);
 /* Scratch bytes, kernels in the graph, and (window, point) entries of a batch
- * (each window padded to a multiple of 32 points). */
+ * (each window padded to a whole number of 4096-point sort tiles). */
 bc_error msm_b200_batch_info(msm_b200_batch batch, size_t *scratch_bytes, unsigned *kernels, unsigned long long *entries);
 bc_error msm_b200_batch_destroy(msm_b200_batch batch);
 

@@ -318,6 +318,24 @@ def test_any_window_and_length(gpu, oracle, window_bits):
     assert oracle.horner(res) == oracle.msm_checksum(k, scalars)
 
 
+@pytest.mark.parametrize("n,window_bits", [(4097, 13), (8191, 15), (12289, 16), (65537, 17), (200003, 17), (131071, 9)])
+def test_sort_tile_edges(gpu, oracle, n, window_bits):
+    """Lengths just past and short of whole sort tiles (4096 keys), skewed
+    scalars (many zero digits, one heavy bucket): the first pass's partial last
+    tile and the look-back passes over windows whose nonzero entries start
+    mid-tile; 9-bit windows take one radix pass, the others two."""
+    scalars, k = synth.workload("skewed", n, 500 + n % 97)
+    bd, _ = generated_bases(gpu, k)
+    sd = gpu.upload(scalars)
+    rd = gpu.bc.malloc(254 * 96)
+    assert gpu.bc.msm_any(gpu.pool, gpu.stream, bd, sd, rd, n, window_bits) == 0
+    gpu.bc.stream_synchronize(gpu.stream)
+    res = gpu.bc.from_device(rd, (254, 24))
+    for p in (bd, sd, rd):
+        gpu.bc.free(p)
+    assert oracle.horner(res) == oracle.msm_checksum(k, scalars)
+
+
 @pytest.mark.parametrize("dist", ["uniform", "skewed"])
 def test_full_size_2_22(gpu, oracle, dist):
     """Configs 1 and 2 (N = 2^22, seeds 1 and 2) against the checksum oracle."""
