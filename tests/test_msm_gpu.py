@@ -452,3 +452,39 @@ def test_reference_parity_2_24(gpu, ref_gpu, oracle):
     gpu.bc.free(bd)
     theirs = oracle.horner(ref_gpu.msm(bases, scalars))
     assert ours == theirs == oracle.msm_checksum(k, scalars)
+
+
+@pytest.mark.parametrize("dist", ["uniform", "skewed"])
+def test_profiled_counts(gpu, oracle, dist):
+    """msm_b200_execute_profiled: the work counts match the digits of the
+    scalars (nonzero entries = W n - zero digits, counted here on the host with
+    the oracle's digit rule), no radix-pass look-back wait gave up, and the
+    result is right."""
+    n = 1 << 16
+    scalars, k = synth.workload(dist, n, 700 + (dist == "skewed"))
+    bd, _ = generated_bases(gpu, k)
+    sd = gpu.upload(scalars)
+    rd = gpu.bc.malloc(254 * 96)
+    prof = gpu.bc.msm_profiled(gpu.pool, gpu.stream, bd, sd, rd, n)
+    res = gpu.bc.from_device(rd, (254, 24))
+    for p in (bd, sd, rd):
+        gpu.bc.free(p)
+    assert prof.sort_wait_timeouts == 0
+    c, windows = prof.window_bits, prof.windows
+    assert windows == (254 + c - 1) // c
+    # signed digits of min(s, r - s) (the fold of the digit kernel), zero digits counted
+    R = H.R
+    unmont = pow(H.MONT, -1, R)
+    zeros = 0
+    for row in scalars:
+        s = H.to_int(row) * unmont % R
+        s = min(s, R - s)
+        carry = 0
+        for w in range(windows):
+            raw = ((s >> (w * c)) & ((1 << c) - 1)) + carry
+            carry = int(raw > (1 << (c - 1)))
+            zeros += int(raw in (0, 1 << c))
+    assert prof.nonzero_entries == windows * n - zeros
+    assert 0 < prof.nonempty_buckets <= windows << (c - 1)
+    assert prof.madds == prof.nonzero_entries - prof.nonempty_buckets - prof.heads
+    assert oracle.horner(res) == oracle.msm_checksum(k, scalars)
