@@ -98,11 +98,14 @@ class MsmB200Profile(ctypes.Structure):
         ("acc_threads", ctypes.c_uint),
         ("launches", ctypes.c_uint),
         ("sort_wait_timeouts", ctypes.c_uint),
+        ("affine_levels", ctypes.c_uint),
+        ("affine_additions", ctypes.c_ulonglong),
     ]
 
     @property
     def madds(self) -> int:
-        return self.nonzero_entries - self.nonempty_buckets - self.heads
+        """XYZZ += affine additions of the accumulation."""
+        return self.nonzero_entries - self.affine_additions - self.nonempty_buckets - self.heads
 
 
 class AffinePoint(ctypes.Structure):
@@ -205,6 +208,7 @@ class BellmanCuda:
                                                   ctypes.POINTER(ctypes.c_uint)],
                 "msm_b200_measure_mul_throughput": [u, ctypes.POINTER(ctypes.c_double)],
                 "msm_b200_execute_no_alloc_async": [Handle, vp, vp, vp, u],
+                "msm_b200_set_affine_levels": [i],
                 "msm_b200_final_sum_async": [vp, vp, Handle],
                 "msm_b200_base_table_create": [ctypes.POINTER(vp), vp, u, ctypes.POINTER(u), u, Handle],
                 "msm_b200_base_table_bytes": [vp, ctypes.POINTER(sz)],
@@ -383,6 +387,10 @@ class BellmanCuda:
         cfg = self._b200_cfg(pool, stream, bases, scalars, results, count, window_bits)
         self.check(self.lib.msm_b200_execute_profiled(ctypes.byref(cfg), ctypes.byref(prof)), "msm_b200_execute_profiled")
         return prof
+
+    def set_affine_levels(self, levels: int) -> None:
+        """Affine pairing levels of later MSMs, process-wide (negative: by size)."""
+        self.check(self.lib.msm_b200_set_affine_levels(levels), "msm_b200_set_affine_levels")
 
     def msm_staged(self, pool: Handle, stream: Handle, bases, scalars, results, count: int, events, window_bits: int = 0) -> int:
         """Enqueue one MSM recording 7 caller events at its stage boundaries; returns kernels launched."""

@@ -228,6 +228,7 @@ __global__ void __launch_bounds__(SORT_THREADS, SORT_SCATTER_MIN_BLOCKS) batch_s
 
 // The batch's segments for accumulate_ranges: one per instance.
 struct table_segments {
+  static constexpr bool POINT_LIST = false;
   const unsigned long long *s_first, *s_end, *s_prefix;
   const uint32_t *s_bucket, *s_mask;
   const affine *const *s_table;

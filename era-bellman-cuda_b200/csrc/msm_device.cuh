@@ -542,6 +542,9 @@ template <int PENDING> __device__ __forceinline__ void cp_async_wait() { asm vol
 //   empty(s)         no nonzero entry
 //   bucket(s, key)   global bucket slot of a key of segment s
 //   base(s, val)     affine base of a value of segment s (sign bit ignored)
+//   POINT_LIST       true for a list of stored points (point_list_segments):
+//                    an entry's value is its own position, no sign, and
+//                    marker points (infinity) are skipped
 template <class SEG>
 __device__ __forceinline__ void accumulate_range(const SEG &seg, const uint32_t *__restrict__ keys, const uint32_t *__restrict__ vals, unsigned t,
                                                  unsigned long long total, unsigned long long active, xyzz *__restrict__ buckets,
@@ -594,17 +597,32 @@ __device__ __forceinline__ void accumulate_range(const SEG &seg, const uint32_t 
       w32[4 * c + 2] = v.z;
       w32[4 * c + 3] = v.w;
     }
-    const fe ny = fq::neg_nonzero(p.y);
-    const bool negative = val >> 31;
+    if constexpr (!SEG::POINT_LIST) {
+      const fe ny = fq::neg_nonzero(p.y);
+      const bool negative = val >> 31;
 #pragma unroll
-    for (int i = 0; i < 8; i++)
-      p.y.l[i] = negative ? ny.l[i] : p.y.l[i];
+      for (int i = 0; i < 8; i++)
+        p.y.l[i] = negative ? ny.l[i] : p.y.l[i];
+    }
     return p;
+  };
+  auto value_at = [&](size_t i) -> uint32_t {
+    if constexpr (SEG::POINT_LIST)
+      return (uint32_t)i;
+    else
+      return vals[i];
+  };
+  // an infinity marker of a point list (x = all ones, never a field element)
+  auto skipped = [&](const affine &p) -> bool {
+    if constexpr (SEG::POINT_LIST)
+      return p.x.l[7] == 0xffffffffu;
+    else
+      return false;
   };
 
   // entry 0 of the range
   uint32_t key = keys[idx];
-  uint32_t val = vals[idx];
+  uint32_t val = value_at(idx);
   issue(0, cw, val);
   // does this range start in the middle of a bucket?
   const bool continued = idx > seg.first(w) && keys[idx - 1] == key;
@@ -616,15 +634,16 @@ __device__ __forceinline__ void accumulate_range(const SEG &seg, const uint32_t 
   if (count > 1) {
     advance();
     nkey = keys[idx];
-    nval = vals[idx];
+    nval = value_at(idx);
     nw = cw;
     issue(1, nw, nval);
     cp_async_wait<1>();
   } else {
     cp_async_wait<0>();
   }
-  xyzz acc = curve::from_affine(fetch(0, val));
-  bool acc_inf = false; // a partial sum can cancel to infinity (p + (-p))
+  const affine p0 = fetch(0, val);
+  xyzz acc = curve::from_affine(p0);
+  bool acc_inf = skipped(p0); // a partial sum can cancel to infinity (p + (-p))
   bool first = true;
   for (unsigned long long k = 1; k < count; k++) {
     key = nkey;
@@ -634,7 +653,7 @@ __device__ __forceinline__ void accumulate_range(const SEG &seg, const uint32_t 
     if (k + 1 < count) {
       advance();
       nkey = keys[idx];
-      nval = vals[idx];
+      nval = value_at(idx);
       nw = cw;
       issue(slot ^ 1, nw, nval);
       cp_async_wait<1>();
@@ -656,11 +675,11 @@ __device__ __forceinline__ void accumulate_range(const SEG &seg, const uint32_t 
       first = false;
       bucket = b;
       acc = curve::from_affine(p);
-      acc_inf = false;
+      acc_inf = skipped(p);
     } else if (acc_inf) {
       acc = curve::from_affine(p);
-      acc_inf = false;
-    } else {
+      acc_inf = skipped(p);
+    } else if (!skipped(p)) {
       acc = curve::add_affine_finite(acc, p, acc_inf);
     }
   }

@@ -15,6 +15,7 @@
 #include "pointer_access.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cstdlib>
 #include <cstring>
 #include <initializer_list>
@@ -46,6 +47,55 @@ unsigned default_window_bits(unsigned long long n) {
     if (lg <= row.max_log_n)
       return row.window_bits;
   return PLAIN_TUNING[sizeof(PLAIN_TUNING) / sizeof(PLAIN_TUNING[0]) - 1].window_bits;
+}
+
+// Affine pairing levels ahead of the XYZZ accumulation (msm_affine.cuh).
+static std::atomic<int> affine_levels_override{-1};
+
+// None by default: measured on a B200 (uniform scalars, kernel times from a
+// launch list), a level's additions cost more than the XYZZ madds they
+// replace.  At 2^22 (c = 17) the first level's forward and apply kernels took
+// 1.72 + 3.73 ms for 31.0 M pair sums (176 ps each: two random gathers of
+// every base, one in each pass), the second level's 0.53 + 1.50 ms for 15.5 M
+// (131 ps), the third's 0.28 + 0.79 ms for 7.7 M, each level's inversion
+// kernel 0.11 ms, against 150 ps per XYZZ += affine addition of the plain
+// accumulation (9.24 ms for 61.8 M); accumulation stage 9.24 ms without
+// levels, 10.28 / 10.08 / 10.12 / 10.21 ms with 1 / 2 / 3 / 4.  At 2^20 (bases
+// in L2) 2.80 ms without, 2.81 / 2.88 / 3.00 / 3.13 ms with 1-4.  The apply
+// kernels run the multiply pipe at 61-74 % (ncu) against the accumulation's
+// 84 %, and every level streams its list through DRAM twice.
+unsigned default_affine_levels(unsigned long long) { return 0; }
+
+void set_affine_levels_override(int levels) { affine_levels_override.store(levels); }
+
+// Upper bound of a level's output elements for m input elements and `slots`
+// buckets: each pair yields one element, or two when its elements belong to
+// different buckets, which happens at most once per bucket boundary.
+static unsigned long long level_output_bound(unsigned long long m, unsigned long long slots) { return std::min(m, (m + 1) / 2 + slots); }
+
+void set_affine_levels(plan &p, unsigned levels) {
+  const unsigned long long entries = (unsigned long long)p.windows * p.n;
+  if (entries >= (1ull << 31))
+    levels = 0; // the XYZZ pass takes list positions as 31-bit entry values
+  p.affine_levels = std::min(levels, MAX_AFFINE_LEVELS);
+  if (!p.affine_levels) {
+    p.level_warps = 0;
+    p.tail_threads = p.acc_threads;
+    p.tail_ranges = p.acc_ranges;
+    return;
+  }
+  const unsigned long long slots = (unsigned long long)p.windows << p.log_b;
+  unsigned long long left = entries;
+  for (unsigned level = 0; level < p.affine_levels; level++)
+    left = level_output_bound(left, slots);
+  const unsigned long long full = (unsigned long long)p.sms * 4 * ACC_THREADS;
+  p.tail_threads = (unsigned)std::max(1ull, std::min(full, (left + 7) / 8));
+  p.tail_ranges = accumulation_ranges(p.tail_threads, left, ACC_RANGES_PER_THREAD);
+  // one resident apply warp per scheduler slot (AFFINE_APPLY_MIN_BLOCKS blocks
+  // per SM), fewer when a lane would have under 16 pairs of the first level
+  const unsigned long long pairs = (entries + 1) / 2;
+  const unsigned long long most = (unsigned long long)p.sms * AFFINE_APPLY_MIN_BLOCKS * (AFFINE_APPLY_THREADS / 32);
+  p.level_warps = (unsigned)std::max(1ull, std::min(most, (pairs + 32 * 16 - 1) / (32 * 16)));
 }
 
 struct device_info {
@@ -102,6 +152,8 @@ plan make_plan(unsigned n, unsigned window_bits, int sms) {
   p.log_m = std::min(3u, p.log_b);
   p.log_g = p.log_b - p.log_m;
   p.groups = 1u << p.log_g;
+  const int forced = affine_levels_override.load();
+  set_affine_levels(p, forced >= 0 ? (unsigned)forced : default_affine_levels(n));
   return p;
 }
 
@@ -207,6 +259,10 @@ static chunking equal_chunks(unsigned n, unsigned max_chunk, bool copy_inputs) {
 struct layout {
   size_t keys[2], vals[2], counts, totals, zeros, sort_ctrs, sort_error, lookback_flags, sort_small_bytes, lookback_agg, lookback_incl, buckets, flags,
       chunk_buckets, chunk_flags, hb[2], hp[2], work, tree[2], streams[2], results, scalars, bases, total;
+  // affine pairing levels: two output lists (level L writes list (L - 1) & 1),
+  // the per-pair prefix products, the per-lane and per-warp arrays, and each
+  // level's output count
+  size_t level_buckets[2], level_points[2], level_pre, level_others, level_total, level_inverse, level_outputs, level_base, level_counts;
 };
 
 static size_t align_up(size_t v) { return (v + 255) & ~(size_t)255; }
@@ -248,9 +304,28 @@ static layout make_layout(const plan &p, bool copy_scalars, bool copy_bases, boo
     l.chunk_buckets = take(slots * sizeof(xyzz));
     l.chunk_flags = take(slots);
   }
+  const size_t heads = std::max(p.acc_ranges, p.tail_ranges);
   for (int i = 0; i < 2; i++) {
-    l.hb[i] = take((size_t)p.acc_ranges * 4);
-    l.hp[i] = take((size_t)p.acc_ranges * sizeof(xyzz));
+    l.hb[i] = take(heads * 4);
+    l.hp[i] = take(heads * sizeof(xyzz));
+  }
+  if (p.affine_levels) {
+    const unsigned long long entries = (unsigned long long)p.windows * p.n, slots = (unsigned long long)p.windows << p.log_b;
+    const unsigned long long first = level_output_bound(entries, slots), second = level_output_bound(first, slots);
+    // later levels shrink: level L's bound is at most that of level L - 2
+    for (int i = 0; i < (p.affine_levels > 1 ? 2 : 1); i++) {
+      const unsigned long long bound = i ? second : first;
+      l.level_buckets[i] = take(bound * 4);
+      l.level_points[i] = take(bound * sizeof(affine));
+    }
+    const size_t warps = p.level_warps;
+    l.level_pre = take((entries + 1) / 2 * sizeof(fe));
+    l.level_others = take(warps * 32 * sizeof(fe));
+    l.level_total = take(warps * sizeof(fe));
+    l.level_inverse = take(warps * sizeof(fe));
+    l.level_outputs = take(warps * 4);
+    l.level_base = take(warps * 8);
+    l.level_counts = take((MAX_AFFINE_LEVELS + 1) * 8);
   }
   l.work = take(sizeof(unsigned));
   for (int i = 0; i < 2; i++) {
@@ -405,17 +480,60 @@ static cudaError_t enqueue_accumulation(const plan &p, const fe *scalars, const 
   // 3. zero digits: counted by the first sort pass (the stage is empty)
   CHECK(m.mark(stream));
 
-  // 4. accumulation
+  // 4. accumulation: the affine pairing levels, if any, then the XYZZ pass
   unsigned *work = reinterpret_cast<unsigned *>(scratch + l.work);
   CHECK(cudaMemsetAsync(work, 0, sizeof(unsigned), stream));
-  accumulate_kernel<<<(p.acc_threads + ACC_THREADS - 1) / ACC_THREADS, ACC_THREADS, 0, stream>>>(
-      keys[cur], vals[cur], bases, n, p.windows, p.log_b, zeros, p.acc_ranges, work, buckets, flags, hb[0], hp[0]);
+  if (p.affine_levels) {
+    uint32_t *list_buckets[2] = {reinterpret_cast<uint32_t *>(scratch + l.level_buckets[0]),
+                                 reinterpret_cast<uint32_t *>(scratch + l.level_buckets[1])};
+    affine *list_points[2] = {reinterpret_cast<affine *>(scratch + l.level_points[0]), reinterpret_cast<affine *>(scratch + l.level_points[1])};
+    unsigned long long *counts_out = reinterpret_cast<unsigned long long *>(scratch + l.level_counts);
+    level_arrays a{};
+    a.pre = reinterpret_cast<fe *>(scratch + l.level_pre);
+    a.others = reinterpret_cast<fe *>(scratch + l.level_others);
+    a.warp_total = reinterpret_cast<fe *>(scratch + l.level_total);
+    a.warp_inverse = reinterpret_cast<fe *>(scratch + l.level_inverse);
+    a.warp_outputs = reinterpret_cast<uint32_t *>(scratch + l.level_outputs);
+    a.warp_base = reinterpret_cast<unsigned long long *>(scratch + l.level_base);
+    const unsigned warps = p.level_warps;
+    const unsigned forward_blocks = (warps * 32 + AFFINE_FORWARD_THREADS - 1) / AFFINE_FORWARD_THREADS;
+    const unsigned apply_blocks = (warps * 32 + AFFINE_APPLY_THREADS - 1) / AFFINE_APPLY_THREADS;
+    for (unsigned level = 1; level <= p.affine_levels; level++) {
+      const int out = (level - 1) & 1, in = level & 1;
+      a.count_out = counts_out + level;
+      a.out_buckets = list_buckets[out];
+      a.out_points = list_points[out];
+      if (level == 1)
+        affine_forward_first_kernel<<<forward_blocks, AFFINE_FORWARD_THREADS, 0, stream>>>(keys[cur], vals[cur], bases, n, p.windows, p.log_b, zeros,
+                                                                                           a, warps);
+      else
+        affine_forward_list_kernel<<<forward_blocks, AFFINE_FORWARD_THREADS, 0, stream>>>(list_buckets[in], list_points[in], counts_out + level - 1,
+                                                                                          a, warps);
+      CHECK(cudaGetLastError());
+      affine_invert_kernel<<<1, AFFINE_INVERT_THREADS, 0, stream>>>(a.warp_total, a.warp_outputs, warps, a.warp_inverse, a.warp_base, a.count_out);
+      CHECK(cudaGetLastError());
+      if (level == 1)
+        affine_apply_first_kernel<<<apply_blocks, AFFINE_APPLY_THREADS, 0, stream>>>(keys[cur], vals[cur], bases, n, p.windows, p.log_b, zeros, a,
+                                                                                       warps);
+      else
+        affine_apply_list_kernel<<<apply_blocks, AFFINE_APPLY_THREADS, 0, stream>>>(list_buckets[in], list_points[in], counts_out + level - 1, a,
+                                                                                     warps);
+      CHECK(cudaGetLastError());
+      m.launched += 3;
+    }
+    const int last = (p.affine_levels - 1) & 1;
+    accumulate_list_kernel<<<(p.tail_threads + ACC_THREADS - 1) / ACC_THREADS, ACC_THREADS, 0, stream>>>(
+        list_buckets[last], list_points[last], counts_out + p.affine_levels, p.tail_ranges, work, buckets, flags, hb[0], hp[0]);
+  } else {
+    accumulate_kernel<<<(p.acc_threads + ACC_THREADS - 1) / ACC_THREADS, ACC_THREADS, 0, stream>>>(
+        keys[cur], vals[cur], bases, n, p.windows, p.log_b, zeros, p.acc_ranges, work, buckets, flags, hb[0], hp[0]);
+  }
   CHECK(cudaGetLastError());
   m.launched++;
   CHECK(m.mark(stream));
 
   // 5. heads
-  unsigned heads = p.acc_ranges;
+  unsigned heads = p.tail_ranges;
   int h = 0;
   while (heads > 1) {
     const unsigned out = (heads + p.merge_chunk - 1) / p.merge_chunk;
@@ -496,8 +614,11 @@ static cudaError_t collect_profile(const plan &p, const layout &l, const uint8_t
   CHECK(cudaMemcpy(&sort_error, scratch + l.sort_error, 4, cudaMemcpyDeviceToHost));
   std::vector<uint8_t> flags((size_t)p.windows << p.log_b);
   CHECK(cudaMemcpy(flags.data(), scratch + l.flags, flags.size(), cudaMemcpyDeviceToHost));
-  std::vector<uint32_t> heads(p.acc_ranges);
+  std::vector<uint32_t> heads(p.tail_ranges);
   CHECK(cudaMemcpy(heads.data(), scratch + l.hb[0], heads.size() * 4, cudaMemcpyDeviceToHost));
+  unsigned long long left = 0; // elements the affine levels left for the XYZZ pass
+  if (p.affine_levels)
+    CHECK(cudaMemcpy(&left, scratch + l.level_counts + p.affine_levels * 8, 8, cudaMemcpyDeviceToHost));
   unsigned long long nonzero = 0, nonempty = 0, continued = 0;
   for (uint32_t z : zeros)
     nonzero += p.n - z;
@@ -510,9 +631,11 @@ static cudaError_t collect_profile(const plan &p, const layout &l, const uint8_t
   out->heads = continued;
   out->window_bits = p.c;
   out->windows = p.windows;
-  out->acc_threads = p.acc_ranges;
+  out->acc_threads = p.tail_ranges;
   out->launches = launches;
   out->sort_wait_timeouts = sort_error;
+  out->affine_levels = p.affine_levels;
+  out->affine_additions = p.affine_levels ? nonzero - left : 0;
   return cudaSuccess;
 }
 
@@ -841,7 +964,8 @@ cudaError_t execute_no_alloc(cudaStream_t stream, const void *bases, const void 
     if (host)
       return cudaErrorInvalidValue;
   }
-  const plan p = make_plan(count, 0, get_device_info(device).sms);
+  plan p = make_plan(count, 0, get_device_info(device).sms);
+  set_affine_levels(p, 0); // the fixed scratch holds no level lists
   const layout l = make_layout(p, false, false, false);
   if (l.total > MSM_B200_NO_ALLOC_SCRATCH_BYTES) // only on GPUs far larger than a B200 (heads grow with the SM count)
     return cudaErrorInvalidValue;
@@ -941,6 +1065,13 @@ bc_error msm_b200_default_window_bits(unsigned count, unsigned *window_bits) {
   if (!window_bits || count == 0)
     return bc_error_invalid_value;
   *window_bits = msm_b200::default_window_bits(count);
+  return bc_success;
+}
+
+bc_error msm_b200_set_affine_levels(int levels) {
+  if (levels > (int)msm_b200::MAX_AFFINE_LEVELS)
+    return bc_error_invalid_value;
+  msm_b200::set_affine_levels_override(levels < 0 ? -1 : levels);
   return bc_success;
 }
 

@@ -56,6 +56,13 @@ cudaError_t enqueue_window_sums(const plan &p, const xyzz *buckets, const uint8_
                                 cudaStream_t stream, unsigned &launched);
 
 unsigned default_window_bits(unsigned long long n);
+// Affine pairing levels by size, and a process-wide override (< 0: by size).
+constexpr unsigned MAX_AFFINE_LEVELS = 4;
+unsigned default_affine_levels(unsigned long long n);
+void set_affine_levels_override(int levels);
+// p with `levels` affine pairing levels (0 for inputs whose list positions
+// would not fit 31 bits), and the geometry of the levels and of the XYZZ pass after them
+void set_affine_levels(plan &p, unsigned levels);
 unsigned accumulation_ranges(unsigned threads, unsigned long long entries, unsigned per_thread);
 plan make_plan(unsigned n, unsigned window_bits, int sms);
 size_t scratch_bytes(unsigned n, unsigned window_bits, bool copy_scalars, bool copy_bases, bool copy_results);

@@ -1,6 +1,6 @@
 // Device kernels of the Pippenger MSM pipeline; see msm_kernels.cuh for the
 // overall data flow.
-#include "msm_device.cuh"
+#include "msm_affine.cuh"
 
 namespace msm_b200 {
 
@@ -189,6 +189,7 @@ constexpr unsigned MAX_WINDOWS = 128;
 // The plain pipeline's segments: window w holds entries [w S, w S + n)
 // (S = window_stride(n)), its nonzero entries last; bucket slot of a key = (w << log_b) | key_slot(key).
 struct window_segments {
+  static constexpr bool POINT_LIST = false;
   const affine *__restrict__ bases;
   const unsigned long long *s_first;  // shared: first nonzero entry of window w, then one past its last
   const unsigned long long *s_prefix; // shared: nonzero entries before window w
@@ -202,14 +203,10 @@ struct window_segments {
   __device__ __forceinline__ const affine *base(unsigned, uint32_t val) const { return bases + (val & 0x7fffffffu); }
 };
 
-__global__ void __launch_bounds__(ACC_THREADS, ACC_MIN_BLOCKS) accumulate_kernel(const uint32_t *__restrict__ keys, const uint32_t *__restrict__ vals,
-                                                                 const affine *__restrict__ bases, unsigned n, unsigned windows, unsigned log_b,
-                                                                 const uint32_t *__restrict__ zeros, unsigned ranges, unsigned *__restrict__ work,
-                                                                 xyzz *__restrict__ buckets, uint8_t *__restrict__ flags,
-                                                                 uint32_t *__restrict__ head_bucket, xyzz *__restrict__ head_point) {
-  __shared__ unsigned long long s_first[2 * MAX_WINDOWS];
-  __shared__ unsigned long long s_prefix[MAX_WINDOWS + 1];
-  __shared__ uint4 s_base[2][4][ACC_THREADS];
+// s_first / s_prefix of window_segments for the n-point windows (zeros[w]
+// zero digits each), filled by the block.
+__device__ __forceinline__ void load_window_segments(unsigned n, unsigned windows, const uint32_t *__restrict__ zeros, unsigned long long *s_first,
+                                                     unsigned long long *s_prefix) {
   const size_t stride = window_stride(n);
   for (unsigned w = threadIdx.x; w < windows; w += blockDim.x) {
     s_first[2 * w] = w * stride + zeros[w];
@@ -225,8 +222,142 @@ __global__ void __launch_bounds__(ACC_THREADS, ACC_MIN_BLOCKS) accumulate_kernel
     s_prefix[windows] = acc;
   }
   __syncthreads();
+}
+
+__global__ void __launch_bounds__(ACC_THREADS, ACC_MIN_BLOCKS) accumulate_kernel(const uint32_t *__restrict__ keys, const uint32_t *__restrict__ vals,
+                                                                 const affine *__restrict__ bases, unsigned n, unsigned windows, unsigned log_b,
+                                                                 const uint32_t *__restrict__ zeros, unsigned ranges, unsigned *__restrict__ work,
+                                                                 xyzz *__restrict__ buckets, uint8_t *__restrict__ flags,
+                                                                 uint32_t *__restrict__ head_bucket, xyzz *__restrict__ head_point) {
+  __shared__ unsigned long long s_first[2 * MAX_WINDOWS];
+  __shared__ unsigned long long s_prefix[MAX_WINDOWS + 1];
+  __shared__ uint4 s_base[2][4][ACC_THREADS];
+  load_window_segments(n, windows, zeros, s_first, s_prefix);
   const window_segments seg{bases, s_first, s_prefix, windows, log_b};
   accumulate_ranges(seg, keys, vals, ranges, work, buckets, flags, head_bucket, head_point, s_base);
+}
+
+// ---------------------------------------------------------------------------
+// 4a. affine pairing levels (msm_affine.cuh)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(AFFINE_FORWARD_THREADS) affine_forward_first_kernel(const uint32_t *__restrict__ keys, const uint32_t *__restrict__ vals,
+                                                                                      const affine *__restrict__ bases, unsigned n, unsigned windows,
+                                                                                      unsigned log_b, const uint32_t *__restrict__ zeros,
+                                                                                      level_arrays a, unsigned warps) {
+  __shared__ unsigned long long s_first[2 * MAX_WINDOWS];
+  __shared__ unsigned long long s_prefix[MAX_WINDOWS + 1];
+  load_window_segments(n, windows, zeros, s_first, s_prefix);
+  const segment_source<window_segments> src{window_segments{bases, s_first, s_prefix, windows, log_b}, keys, vals};
+  affine_forward(src, a, warps);
+}
+
+__global__ void __launch_bounds__(AFFINE_APPLY_THREADS, AFFINE_APPLY_MIN_BLOCKS) affine_apply_first_kernel(
+    const uint32_t *__restrict__ keys, const uint32_t *__restrict__ vals, const affine *__restrict__ bases, unsigned n, unsigned windows,
+    unsigned log_b, const uint32_t *__restrict__ zeros, level_arrays a, unsigned warps) {
+  __shared__ unsigned long long s_first[2 * MAX_WINDOWS];
+  __shared__ unsigned long long s_prefix[MAX_WINDOWS + 1];
+  load_window_segments(n, windows, zeros, s_first, s_prefix);
+  const segment_source<window_segments> src{window_segments{bases, s_first, s_prefix, windows, log_b}, keys, vals};
+  affine_apply(src, a, warps);
+}
+
+__global__ void __launch_bounds__(AFFINE_FORWARD_THREADS) affine_forward_list_kernel(const uint32_t *__restrict__ list_buckets,
+                                                                                     const affine *__restrict__ points,
+                                                                                     const unsigned long long *__restrict__ count, level_arrays a,
+                                                                                     unsigned warps) {
+  const list_source src{list_buckets, points, *count};
+  affine_forward(src, a, warps);
+}
+
+__global__ void __launch_bounds__(AFFINE_APPLY_THREADS, AFFINE_APPLY_MIN_BLOCKS) affine_apply_list_kernel(const uint32_t *__restrict__ list_buckets,
+                                                                                                          const affine *__restrict__ points,
+                                                                                                          const unsigned long long *__restrict__ count,
+                                                                                                          level_arrays a, unsigned warps) {
+  const list_source src{list_buckets, points, *count};
+  affine_apply(src, a, warps);
+}
+
+// Thread t takes warps [t E, (t + 1) E): its own product chain over their
+// totals (warp_inverse holds each one's prefix meanwhile), then the block's
+// products of the other threads' chains (warp_products within each warp, then
+// across the warps), one inversion of the block total by the binary extended
+// Euclidean algorithm, and the chain backwards.  The output counts are scanned
+// in the same arrangement.
+__global__ void __launch_bounds__(AFFINE_INVERT_THREADS) affine_invert_kernel(const fe *__restrict__ warp_total, const uint32_t *__restrict__ warp_outputs,
+                                                                              unsigned warps, fe *__restrict__ warp_inverse,
+                                                                              unsigned long long *__restrict__ warp_base,
+                                                                              unsigned long long *__restrict__ count_out) {
+  constexpr unsigned WARPS = AFFINE_INVERT_THREADS / 32;
+  __shared__ fe s_total[WARPS], s_others[WARPS];
+  __shared__ fe s_inverse;
+  __shared__ unsigned long long s_sum[WARPS];
+  const unsigned t = threadIdx.x, lane = t & 31, wid = t >> 5;
+  const unsigned per = (warps + AFFINE_INVERT_THREADS - 1) / AFFINE_INVERT_THREADS;
+  const unsigned beg = min(warps, t * per), end = min(warps, beg + per);
+  fe acc = fq::one();
+  unsigned long long sum = 0;
+  for (unsigned j = beg; j < end; j++) {
+    store_fe(warp_inverse + j, acc);
+    acc = fq::mul(acc, warp_total[j]);
+    sum += warp_outputs[j];
+  }
+  fe others, total;
+  warp_products(acc, &others, &total);
+  unsigned long long incl = sum; // inclusive scan of the counts within the warp
+#pragma unroll
+  for (unsigned d = 1; d < 32; d <<= 1) {
+    const unsigned long long v = __shfl_up_sync(0xffffffffu, incl, d);
+    if (lane >= d)
+      incl += v;
+  }
+  if (lane == 31) {
+    s_total[wid] = total;
+    s_sum[wid] = incl;
+  }
+  __syncthreads();
+  if (wid == 0) {
+    fe o, all;
+    warp_products(lane < WARPS ? s_total[lane] : fq::one(), &o, &all);
+    const unsigned long long c = lane < WARPS ? s_sum[lane] : 0;
+    unsigned long long ci = c;
+#pragma unroll
+    for (unsigned d = 1; d < 32; d <<= 1) {
+      const unsigned long long v = __shfl_up_sync(0xffffffffu, ci, d);
+      if (lane >= d)
+        ci += v;
+    }
+    if (lane < WARPS) {
+      s_others[lane] = o;
+      s_sum[lane] = ci - c;
+    }
+    if (lane == WARPS - 1)
+      *count_out = ci;
+    if (lane == 0)
+      s_inverse = fq::to_mont(fq::inverse_binary(fq::from_mont(all)));
+  }
+  __syncthreads();
+  fe inv = fq::mul(fq::mul(s_inverse, s_others[wid]), others);
+  for (unsigned j = end; j-- > beg;) {
+    const fe pre = warp_inverse[j];
+    warp_inverse[j] = fq::mul(inv, pre);
+    inv = fq::mul(inv, warp_total[j]);
+  }
+  unsigned long long base = s_sum[wid] + incl - sum;
+  for (unsigned j = beg; j < end; j++) {
+    warp_base[j] = base;
+    base += warp_outputs[j];
+  }
+}
+
+__global__ void __launch_bounds__(ACC_THREADS, ACC_MIN_BLOCKS) accumulate_list_kernel(const uint32_t *__restrict__ list_buckets,
+                                                                                      const affine *__restrict__ points,
+                                                                                      const unsigned long long *__restrict__ count, unsigned ranges,
+                                                                                      unsigned *__restrict__ work, xyzz *__restrict__ buckets,
+                                                                                      uint8_t *__restrict__ flags, uint32_t *__restrict__ head_bucket,
+                                                                                      xyzz *__restrict__ head_point) {
+  __shared__ uint4 s_base[2][4][ACC_THREADS];
+  const point_list_segments seg{points, *count};
+  accumulate_ranges(seg, list_buckets, nullptr, ranges, work, buckets, flags, head_bucket, head_point, s_base);
 }
 
 // ---------------------------------------------------------------------------

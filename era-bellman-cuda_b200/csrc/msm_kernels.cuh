@@ -83,6 +83,10 @@ struct plan {
   unsigned groups;      // G = B / m groups per window
   unsigned log_g;       // gamma = log2 G
   unsigned sms;         // SMs of the device the plan is for
+  unsigned affine_levels; // affine pairing levels before the XYZZ accumulation (0: none)
+  unsigned level_warps;   // warps of each level's grid
+  unsigned tail_threads;  // XYZZ accumulation threads and ranges after the levels
+  unsigned tail_ranges;
 };
 
 // ---------------------------------------------------------------------------
@@ -133,6 +137,47 @@ __global__ void accumulate_kernel(const uint32_t *__restrict__ keys, const uint3
                                   unsigned n, unsigned windows, unsigned log_b, const uint32_t *__restrict__ zeros, unsigned ranges,
                                   unsigned *__restrict__ work, xyzz *__restrict__ buckets, uint8_t *__restrict__ flags,
                                   uint32_t *__restrict__ head_bucket, xyzz *__restrict__ head_point);
+
+// Affine pairing levels ahead of the accumulation (msm_affine.cuh).
+constexpr unsigned AFFINE_FORWARD_THREADS = 256;
+constexpr unsigned AFFINE_APPLY_THREADS = 128;
+constexpr unsigned AFFINE_INVERT_THREADS = 512;
+#ifndef AFFINE_APPLY_MIN_BLOCKS
+#define AFFINE_APPLY_MIN_BLOCKS 4 // resident apply blocks per SM (caps registers at 128)
+#endif
+// Per-level arrays of a grid of `warps` warps:
+struct level_arrays {
+  fe *pre;                       // per pair: product of the lane's earlier slope denominators
+  fe *others;                    // per lane: product of the other lanes' chain totals
+  fe *warp_total;                // per warp: product of all its slope denominators
+  fe *warp_inverse;              // per warp: inverse of warp_total
+  uint32_t *warp_outputs;        // per warp: output elements
+  unsigned long long *warp_base; // per warp: position of its first output element
+  unsigned long long *count_out; // output elements of the level
+  uint32_t *out_buckets;         // output list: global bucket ids and points
+  affine *out_points;
+};
+// level 1 over the sorted nonzero entries of the windows (as accumulate_kernel reads them)
+__global__ void affine_forward_first_kernel(const uint32_t *__restrict__ keys, const uint32_t *__restrict__ vals, const affine *__restrict__ bases,
+                                            unsigned n, unsigned windows, unsigned log_b, const uint32_t *__restrict__ zeros, level_arrays a,
+                                            unsigned warps);
+__global__ void affine_apply_first_kernel(const uint32_t *__restrict__ keys, const uint32_t *__restrict__ vals, const affine *__restrict__ bases,
+                                          unsigned n, unsigned windows, unsigned log_b, const uint32_t *__restrict__ zeros, level_arrays a,
+                                          unsigned warps);
+// later levels over the previous level's list of *count elements
+__global__ void affine_forward_list_kernel(const uint32_t *__restrict__ list_buckets, const affine *__restrict__ points,
+                                           const unsigned long long *__restrict__ count, level_arrays a, unsigned warps);
+__global__ void affine_apply_list_kernel(const uint32_t *__restrict__ list_buckets, const affine *__restrict__ points,
+                                         const unsigned long long *__restrict__ count, level_arrays a, unsigned warps);
+// one block: warp_inverse, warp_base and *count_out of a level
+__global__ void affine_invert_kernel(const fe *__restrict__ warp_total, const uint32_t *__restrict__ warp_outputs, unsigned warps,
+                                     fe *__restrict__ warp_inverse, unsigned long long *__restrict__ warp_base,
+                                     unsigned long long *__restrict__ count_out);
+// the XYZZ accumulation over the last level's list of *count elements
+__global__ void accumulate_list_kernel(const uint32_t *__restrict__ list_buckets, const affine *__restrict__ points,
+                                       const unsigned long long *__restrict__ count, unsigned ranges, unsigned *__restrict__ work,
+                                       xyzz *__restrict__ buckets, uint8_t *__restrict__ flags, uint32_t *__restrict__ head_bucket,
+                                       xyzz *__restrict__ head_point);
 
 // ---------------------------------------------------------------------------
 // 5. heads

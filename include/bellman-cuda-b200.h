@@ -38,12 +38,26 @@ typedef struct msm_b200_profile {
   unsigned long long heads;            /* accumulation ranges that began inside a bucket */
   unsigned window_bits, windows, acc_threads /* accumulation ranges */, launches;
   unsigned sort_wait_timeouts; /* radix-pass look-back waits that gave up (0 in correct operation) */
+  unsigned affine_levels;                /* affine pairing levels run before the XYZZ accumulation */
+  unsigned long long affine_additions;   /* list elements those levels removed (one per affine pair sum) */
 } msm_b200_profile;
 
 /* Same as msm_b200_execute_async, but synchronises the stream before it
- * returns and fills *profile.  Mixed additions performed by the accumulation
- * kernel = nonzero_entries - nonempty_buckets - heads. */
+ * returns and fills *profile.  Mixed (XYZZ += affine) additions performed by
+ * the accumulation = nonzero_entries - affine_additions - nonempty_buckets -
+ * heads. */
 bc_error msm_b200_execute_profiled(const msm_b200_configuration *configuration, msm_b200_profile *profile);
+
+/* Affine pairing levels of later calls, process-wide: 0..4 levels for every
+ * size, or a negative value for the default (none).  Each level adds, in
+ * affine coordinates, every two consecutive sorted entries of one bucket, all
+ * of a level's slopes sharing one field inversion (5 products and 1 square per
+ * addition against the XYZZ madd's 8 and 2); the XYZZ accumulation then adds
+ * what is left.  Results are the same group elements either way.  On a B200
+ * the levels measure slower than the XYZZ pass at every size (each level
+ * streams its list through memory twice, and the first gathers every base
+ * twice), hence the default. */
+bc_error msm_b200_set_affine_levels(int levels);
 
 /* msm_b200_execute_async that also records stage_events[0..6] on the stream:
  * before the first stage and after each of the six stages of
