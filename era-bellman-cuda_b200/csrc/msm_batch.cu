@@ -631,8 +631,8 @@ cudaError_t enqueue_batch(const batch_plan &b, uint8_t *scratch, cudaStream_t s,
   unsigned heads = b.acc_ranges;
   int h = 0;
   while (heads > 1) {
-    const unsigned out = (heads + 3) / 4;
-    merge_heads_kernel<<<(out + ACC_THREADS - 1) / ACC_THREADS, ACC_THREADS, 0, s>>>(hb[h], hp[h], heads, 4, buckets, hb[h ^ 1], hp[h ^ 1]);
+    const unsigned out = (heads + MERGE_HEADS_PER_WARP - 1) / MERGE_HEADS_PER_WARP;
+    merge_heads_kernel<<<(out * 32 + ACC_THREADS - 1) / ACC_THREADS, ACC_THREADS, 0, s>>>(hb[h], hp[h], heads, buckets, hb[h ^ 1], hp[h ^ 1]);
     CHECK(cudaGetLastError());
     launched++;
     heads = out;

@@ -147,7 +147,6 @@ plan make_plan(unsigned n, unsigned window_bits, int sms) {
   const unsigned long long full = (unsigned long long)sms * 4 * ACC_THREADS;
   p.acc_threads = (unsigned)std::max(1ull, std::min(full, (entries + 7) / 8));
   p.acc_ranges = accumulation_ranges(p.acc_threads, entries, ACC_RANGES_PER_THREAD);
-  p.merge_chunk = 4;
   // groups of m = 8 slots: enough reduction threads to fill the GPU at c = 16
   p.log_m = std::min(3u, p.log_b);
   p.log_g = p.log_b - p.log_m;
@@ -417,7 +416,7 @@ static cudaError_t enqueue_accumulation(const plan &p, const fe *scalars, const 
   unsigned *sort_error = reinterpret_cast<unsigned *>(scratch + l.sort_error);
   CHECK(cudaMemsetAsync(totals, 0, l.sort_small_bytes, stream));
   int cur = 0;
-  if (p.windows <= MAX_FUSED_HISTOGRAM_WINDOWS) {
+  if (p.windows <= MAX_FUSED_HISTOGRAM_WINDOWS && p.tiles >= FUSED_DIGITS_MIN_TILES) {
     // 1. digits, with every pass's digit counts per tile
     digits_histogram_kernel<<<p.tiles, SORT_THREADS, digit_histogram_smem(p.windows, p.sort_passes), stream>>>(
         scalars, n, p.c, p.windows, p.sort_passes, p.tiles, keys[0], vals[0], counts, totals, zeros);
@@ -536,9 +535,8 @@ static cudaError_t enqueue_accumulation(const plan &p, const fe *scalars, const 
   unsigned heads = p.tail_ranges;
   int h = 0;
   while (heads > 1) {
-    const unsigned out = (heads + p.merge_chunk - 1) / p.merge_chunk;
-    merge_heads_kernel<<<(out + ACC_THREADS - 1) / ACC_THREADS, ACC_THREADS, 0, stream>>>(hb[h], hp[h], heads, p.merge_chunk, buckets,
-                                                                                           hb[h ^ 1], hp[h ^ 1]);
+    const unsigned out = (heads + MERGE_HEADS_PER_WARP - 1) / MERGE_HEADS_PER_WARP;
+    merge_heads_kernel<<<(out * 32 + ACC_THREADS - 1) / ACC_THREADS, ACC_THREADS, 0, stream>>>(hb[h], hp[h], heads, buckets, hb[h ^ 1], hp[h ^ 1]);
     CHECK(cudaGetLastError());
     m.launched++;
     heads = out;

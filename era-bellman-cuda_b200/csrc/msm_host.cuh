@@ -30,6 +30,16 @@ struct execution {
 
 // windows whose first-pass histograms the digit kernel builds in shared memory
 constexpr unsigned MAX_FUSED_HISTOGRAM_WINDOWS = 48;
+// Sort tiles below which the unfused path (a digit kernel of one thread per
+// point, then histogram + scan + scatter per pass) runs instead: the fused
+// digit kernel has one block per tile, too few blocks to fill the GPU.
+// Measured on a B200 (plain MSM, default widths): unfused faster up to 2^18
+// points (64 tiles; 2^14 at c = 8 0.579 -> 0.466 ms, 2^16 0.683 -> 0.653 ms,
+// 2^18 1.217 -> 1.200 ms), fused faster from 2^19 (128 tiles: 1.984 against
+// 1.997 ms; 2^20 3.500 against 3.581 ms).
+#ifndef FUSED_DIGITS_MIN_TILES
+#define FUSED_DIGITS_MIN_TILES 128
+#endif
 
 // stages timed by msm_b200_execute_profiled
 constexpr unsigned PROFILE_STAGES = 6;

@@ -363,48 +363,61 @@ __global__ void __launch_bounds__(ACC_THREADS, ACC_MIN_BLOCKS) accumulate_list_k
 // ---------------------------------------------------------------------------
 // 5. fold head partial sums into their buckets
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ xyzz shfl_up_xyzz(const xyzz &v, unsigned delta) {
+  xyzz r;
+  const uint32_t *a = reinterpret_cast<const uint32_t *>(&v);
+  uint32_t *b = reinterpret_cast<uint32_t *>(&r);
+#pragma unroll
+  for (int i = 0; i < 32; i++)
+    b[i] = __shfl_up_sync(0xffffffffu, a[i], delta);
+  return r;
+}
+
+// Warp w takes heads [32 w, 32 w + 32): a segmented inclusive scan over the
+// lanes (Kogge-Stone, five shuffle steps; the heads of one bucket are
+// contiguous, so equal buckets at distance d mean one segment in between)
+// leaves each segment's sum in its last lane.  A segment whose bucket also
+// holds the head before the warp's first is a continuation and becomes the
+// warp's output head; every other segment holds its bucket's first heads of
+// this level and is added into the bucket (no other warp of the launch
+// touches that bucket).  All lanes take every shuffle before any diverges.
 __global__ void __launch_bounds__(ACC_THREADS) merge_heads_kernel(const uint32_t *__restrict__ hb_in, const xyzz *__restrict__ hp_in,
-                                                                  unsigned n_in, unsigned chunk, xyzz *__restrict__ buckets,
-                                                                  uint32_t *__restrict__ hb_out, xyzz *__restrict__ hp_out) {
-  const unsigned u = blockIdx.x * blockDim.x + threadIdx.x;
-  const unsigned long long beg = (unsigned long long)u * chunk;
-  if (beg >= n_in)
-    return;
-  const unsigned end = (unsigned)min((unsigned long long)n_in, beg + chunk);
-  hb_out[u] = INVALID_BUCKET;
-  unsigned bucket = INVALID_BUCKET;
-  bool head_is_continuation = false, seen = false;
-  xyzz acc;
-  for (unsigned k = (unsigned)beg; k < end; k++) {
-    const unsigned b = hb_in[k];
-    if (b == INVALID_BUCKET)
-      continue;
-    const xyzz p = load_xyzz(hp_in + k);
-    if (b != bucket) {
-      if (bucket != INVALID_BUCKET) {
-        if (head_is_continuation) {
-          hb_out[u] = bucket;
-          store_xyzz(hp_out + u, acc);
-        } else {
-          store_xyzz(buckets + bucket, curve::add(load_xyzz(buckets + bucket), acc));
-        }
-      }
-      head_is_continuation = !seen && k == beg && k > 0 && hb_in[k - 1] == b;
-      seen = true;
-      bucket = b;
-      acc = p;
+                                                                  unsigned n_in, xyzz *__restrict__ buckets, uint32_t *__restrict__ hb_out,
+                                                                  xyzz *__restrict__ hp_out) {
+  const unsigned lane = threadIdx.x & 31;
+  const unsigned w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if ((unsigned long long)w * 32 >= n_in)
+    return; // whole warps only
+  const unsigned long long k = (unsigned long long)w * 32 + lane;
+  const uint32_t b = k < n_in ? hb_in[k] : INVALID_BUCKET;
+  xyzz acc = b != INVALID_BUCKET ? load_xyzz(hp_in + k) : curve::infinity();
+#pragma unroll
+  for (unsigned d = 1; d < 32; d <<= 1) {
+    const uint32_t bo = __shfl_up_sync(0xffffffffu, b, d);
+    const xyzz o = shfl_up_xyzz(acc, d);
+    if (lane >= d && bo == b && b != INVALID_BUCKET)
+      acc = curve::add(o, acc);
+  }
+  const uint32_t prev = __shfl_up_sync(0xffffffffu, b, 1), next = __shfl_down_sync(0xffffffffu, b, 1);
+  const unsigned joins = __ballot_sync(0xffffffffu, lane > 0 && prev == b); // lane continues lane - 1's segment
+  const unsigned first = 31 - __clz(~joins & ((2u << lane) - 1));          // first lane of this lane's segment
+  const uint32_t b0 = __shfl_sync(0xffffffffu, b, 0);
+  uint32_t before = INVALID_BUCKET;
+  if (lane == 0 && w > 0)
+    before = hb_in[(size_t)w * 32 - 1];
+  before = __shfl_sync(0xffffffffu, before, 0);
+  const bool continued = b0 != INVALID_BUCKET && before == b0; // lane 0's segment began in an earlier warp
+  const bool last = lane == 31 || next != b;
+  if (b != INVALID_BUCKET && last) {
+    if (first == 0 && continued) {
+      hb_out[w] = b;
+      store_xyzz(hp_out + w, acc);
     } else {
-      acc = curve::add(acc, p);
+      store_xyzz(buckets + b, curve::add(load_xyzz(buckets + b), acc));
     }
   }
-  if (bucket != INVALID_BUCKET) {
-    if (head_is_continuation) {
-      hb_out[u] = bucket;
-      store_xyzz(hp_out + u, acc);
-    } else {
-      store_xyzz(buckets + bucket, curve::add(load_xyzz(buckets + bucket), acc));
-    }
-  }
+  if (lane == 0 && !continued)
+    hb_out[w] = INVALID_BUCKET;
 }
 
 // Fold the buckets of one chunk of points into the MSM's buckets (host-resident

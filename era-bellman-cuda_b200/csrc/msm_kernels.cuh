@@ -78,7 +78,6 @@ struct plan {
   unsigned tiles;       // sort tiles per window
   unsigned acc_threads; // accumulation threads (4 blocks of ACC_THREADS per SM at most)
   unsigned acc_ranges;  // accumulation ranges (>= acc_threads), handed out to warps
-  unsigned merge_chunk; // heads per merge thread
   unsigned log_m;       // log2 of the running-sum group
   unsigned groups;      // G = B / m groups per window
   unsigned log_g;       // gamma = log2 G
@@ -182,8 +181,10 @@ __global__ void accumulate_list_kernel(const uint32_t *__restrict__ list_buckets
 // ---------------------------------------------------------------------------
 // 5. heads
 // ---------------------------------------------------------------------------
-__global__ void merge_heads_kernel(const uint32_t *__restrict__ hb_in, const xyzz *__restrict__ hp_in, unsigned n_in, unsigned chunk,
-                                   xyzz *__restrict__ buckets, uint32_t *__restrict__ hb_out, xyzz *__restrict__ hp_out);
+// 32 heads per warp; one output head per warp (hb_out[w], INVALID_BUCKET if none)
+constexpr unsigned MERGE_HEADS_PER_WARP = 32;
+__global__ void merge_heads_kernel(const uint32_t *__restrict__ hb_in, const xyzz *__restrict__ hp_in, unsigned n_in, xyzz *__restrict__ buckets,
+                                   uint32_t *__restrict__ hb_out, xyzz *__restrict__ hp_out);
 
 // buckets += chunk_buckets for every slot flagged in chunk_flags
 __global__ void merge_chunk_buckets_kernel(xyzz *__restrict__ buckets, uint8_t *__restrict__ flags, const xyzz *__restrict__ chunk_buckets,

@@ -176,4 +176,6 @@ def test_c_caller_links_and_runs_without_a_gpu(product_lib_path, tmp_path):
     subprocess.run(["gcc", "-std=c11", "-I", INCLUDE, str(src), "-L", libdir, "-lbellman_cuda_b200", "-Wl,-rpath," + libdir, "-o", str(exe)],
                    check=True)
     out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()
-    assert out == ["1", "1", "1", "0", "15"]
+    table = open(os.path.join(os.path.dirname(INCLUDE), "era-bellman-cuda_b200", "csrc", "plain_tuning.h")).read()
+    width_2_20 = re.search(r"\{20, (\d+)\}", table).group(1)  # the measured width at 2^20 points
+    assert out == ["1", "1", "1", "0", width_2_20]

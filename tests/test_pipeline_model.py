@@ -1,6 +1,6 @@
 """Integer model of the GPU pipeline's decomposition (a point is its discrete
 log mod r): signed digits of min(s, r - s), stable per-window sort, equal
-ranges with head partial sums, chunked head merging, grouped running sums and
+ranges with head partial sums, warp-segmented head merging, grouped running sums and
 the binary decomposition that places every partial sum at its bit of the
 254-entry result.  Checks sum_i 2^i R_i == sum_i k_i s_i, and that no partial
 sum lands above bit 253.  Mirrors era-bellman-cuda_b200/csrc/msm_kernels.cu."""
@@ -16,7 +16,42 @@ def key_slot(key, B):
     return (key + 1) & (B - 1)
 
 
-def model_msm(scal, kl, c, T, chunk=4, log_m_max=3):
+def merge_heads_level(hb, hp, heads, buckets):
+    """One merge_heads_kernel launch, lane by lane: warp w takes heads
+    [32 w, 32 w + 32), a segmented Kogge-Stone inclusive scan leaves each
+    segment's sum in its last lane; the segment holding lane 0 is a
+    continuation when the head before the warp has its bucket (-> the warp's
+    output head), every other segment is added into its bucket."""
+    out = (heads + 31) // 32
+    hb2, hp2 = [None] * out, [0] * out
+    updated = set()
+    for w in range(out):
+        b = [hb[32 * w + l] if 32 * w + l < heads else None for l in range(32)]
+        acc = [hp[32 * w + l] if b[l] is not None else 0 for l in range(32)]
+        d = 1
+        while d < 32:
+            old = list(acc)  # every lane shuffles before any adds
+            for l in range(32):
+                if l >= d and b[l - d] == b[l] and b[l] is not None:
+                    acc[l] = (old[l - d] + old[l]) % R
+            d <<= 1
+        joins = [l > 0 and b[l - 1] == b[l] for l in range(32)]
+        before = hb[32 * w - 1] if w > 0 else None
+        continued = b[0] is not None and before == b[0]
+        for l in range(32):
+            if b[l] is None or (l < 31 and b[l + 1] == b[l]):
+                continue
+            first = max(f for f in range(l + 1) if not joins[f])
+            if first == 0 and continued:
+                hb2[w], hp2[w] = b[l], acc[l]
+            else:
+                assert b[l] not in updated, "two segments of one launch update one bucket"
+                updated.add(b[l])
+                buckets[b[l]] = (buckets[b[l]] + acc[l]) % R
+    return hb2, hp2
+
+
+def model_msm(scal, kl, c, T, log_m_max=3):
     n = len(scal)
     W = (254 + c - 1) // c
     log_b = c - 1
@@ -93,35 +128,8 @@ def model_msm(scal, kl, c, T, chunk=4, log_m_max=3):
         for a, b in zip(valid, valid[1:]):
             if hb[a] == hb[b]:
                 assert b == a + 1, "heads of one bucket are not contiguous"
-        out = (heads + chunk - 1) // chunk
-        hb2, hp2 = [None] * out, [0] * out
-        updated = set()
-        for u in range(out):
-            beg, end = u * chunk, min(heads, u * chunk + chunk)
-            bucket, isc, seen, acc = None, False, False, 0
-            for k in range(beg, end):
-                b = hb[k]
-                if b is None:
-                    continue
-                if b != bucket:
-                    if bucket is not None:
-                        if isc:
-                            hb2[u], hp2[u] = bucket, acc
-                        else:
-                            assert bucket not in updated
-                            updated.add(bucket)
-                            buckets[bucket] = (buckets[bucket] + acc) % R
-                    isc = (not seen) and k == beg and k > 0 and hb[k - 1] == b
-                    seen, bucket, acc = True, b, hp[k]
-                else:
-                    acc = (acc + hp[k]) % R
-            if bucket is not None:
-                if isc:
-                    hb2[u], hp2[u] = bucket, acc
-                else:
-                    assert bucket not in updated
-                    updated.add(bucket)
-                    buckets[bucket] = (buckets[bucket] + acc) % R
+        hb2, hp2 = merge_heads_level(hb, hp, heads, buckets)
+        out = len(hb2)
         hb, hp, heads = hb2, hp2, out
     log_m = min(log_m_max, log_b)
     log_g = log_b - log_m
@@ -214,3 +222,19 @@ def test_final_sum_tree(trial):
     rng = random.Random(2000 + trial)
     values = [rng.randrange(R) if rng.random() < 0.8 else 0 for _ in range(254)]
     assert model_final_sum(values) == sum(v * pow(2, i, R) for i, v in enumerate(values)) % R
+
+
+@pytest.mark.parametrize("n,c,T,mode", [(2000, 4, 1500, "one"), (700, 2, 3000, "uniform"), (1200, 3, 1100, "skewed"),
+                                        (64, 2, 5000, "uniform")])
+def test_model_many_heads(n, c, T, mode):
+    """Many heads per bucket: a bucket's heads span several warps of the merge
+    and several merge levels (all scalars 1 puts every entry in one bucket)."""
+    rng = random.Random(n * 31 + T)
+    if mode == "one":
+        scal = [1] * n
+    elif mode == "uniform":
+        scal = [rng.randrange(R) for _ in range(n)]
+    else:
+        scal = [rng.choice([0, 1, 1, 2, rng.randrange(R)]) for _ in range(n)]
+    kl = [rng.randrange(1, R) for _ in range(n)]
+    assert model_msm(scal, kl, c, T) == sum(s * k for s, k in zip(scal, kl)) % R
