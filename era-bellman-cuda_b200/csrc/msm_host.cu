@@ -131,6 +131,24 @@ unsigned accumulation_ranges(unsigned threads, unsigned long long entries, unsig
   return (unsigned)(threads * k);
 }
 
+// log2 of the running-sum group of the reduction per window width.  A group
+// thread's 2 (m - 1) additions are one dependent chain, so few buckets want
+// small groups (the chain is the stage's latency), many buckets larger ones
+// (fewer tree levels).  Measured on a B200, reduction stage with m = 8 / 4 / 2:
+// c = 5 (2^12 points) 0.110 / 0.079 / 0.067 ms, c = 11 (2^14) 0.198 / 0.159 /
+// 0.145, c = 13 (2^16) 0.226 / 0.198 / 0.194, c = 15 (2^18) 0.290 / 0.312 /
+// 0.319, c = 16 (2^20) 0.445 / 0.433 / 0.435, c = 17 (2^22) 0.664 / 0.637 /
+// 0.656.
+static unsigned reduction_log_m(unsigned c) { return c <= 14 ? 1 : c == 15 ? 3 : 2; }
+
+// Groups of 2^log_m slots (at most the window's slots); the reduction's tree
+// and stream buffers hold G = 2^(log_b - log_m) entries per window.
+static void set_reduction_groups(plan &p, unsigned log_m) {
+  p.log_m = std::min(log_m, p.log_b);
+  p.log_g = p.log_b - p.log_m;
+  p.groups = 1u << p.log_g;
+}
+
 plan make_plan(unsigned n, unsigned window_bits, int sms) {
   plan p{};
   p.n = n;
@@ -147,10 +165,7 @@ plan make_plan(unsigned n, unsigned window_bits, int sms) {
   const unsigned long long full = (unsigned long long)sms * 4 * ACC_THREADS;
   p.acc_threads = (unsigned)std::max(1ull, std::min(full, (entries + 7) / 8));
   p.acc_ranges = accumulation_ranges(p.acc_threads, entries, ACC_RANGES_PER_THREAD);
-  // groups of m = 8 slots: enough reduction threads to fill the GPU at c = 16
-  p.log_m = std::min(3u, p.log_b);
-  p.log_g = p.log_b - p.log_m;
-  p.groups = 1u << p.log_g;
+  set_reduction_groups(p, reduction_log_m(p.c));
   const int forced = affine_levels_override.load();
   set_affine_levels(p, forced >= 0 ? (unsigned)forced : default_affine_levels(n));
   return p;
@@ -963,7 +978,8 @@ cudaError_t execute_no_alloc(cudaStream_t stream, const void *bases, const void 
       return cudaErrorInvalidValue;
   }
   plan p = make_plan(count, 0, get_device_info(device).sms);
-  set_affine_levels(p, 0); // the fixed scratch holds no level lists
+  set_affine_levels(p, 0);   // the fixed scratch holds no level lists
+  set_reduction_groups(p, 3); // and the reduction's smallest tree (G = B / 8)
   const layout l = make_layout(p, false, false, false);
   if (l.total > MSM_B200_NO_ALLOC_SCRATCH_BYTES) // only on GPUs far larger than a B200 (heads grow with the SM count)
     return cudaErrorInvalidValue;
