@@ -13,8 +13,11 @@
 //                  range bucket by bucket (XYZZ += affine); buckets that start
 //                  inside a range are written directly, a bucket continued
 //                  from the previous range leaves a "head" partial sum
-//   5. merge_heads heads of one bucket are contiguous; chunked, repeated
-//                  until every head is folded into its bucket
+//                  (optionally preceded by affine pairing levels, off by
+//                  default: msm_affine.cuh)
+//   5. merge_heads heads of one bucket are contiguous; a segmented scan of 32
+//                  heads per warp, repeated until every head is folded into
+//                  its bucket
 //   6. reduction   per window S_w = sum_k k * X_k (X_k = bucket of |d| = k,
 //                  slot 0 holds |d| = B): running sums over groups of m slots,
 //                  then a binary decomposition of the group weights, so every
