@@ -48,8 +48,10 @@ typedef struct msm_b200_profile {
  * heads. */
 bc_error msm_b200_execute_profiled(const msm_b200_configuration *configuration, msm_b200_profile *profile);
 
-/* Affine pairing levels of later calls, process-wide: 0..4 levels for every
- * size, or a negative value for the default (none).  Each level adds, in
+/* Affine pairing levels of later plain MSMs (msm_execute_async and the
+ * msm_b200_execute_* calls; the batched path and the server do not use
+ * them), process-wide: 0..4 levels for every size, or a negative value for
+ * the default (none).  Each level adds, in
  * affine coordinates, every two consecutive sorted entries of one bucket, all
  * of a level's slopes sharing one field inversion (5 products and 1 square per
  * addition against the XYZZ madd's 8 and 2); the XYZZ accumulation then adds

@@ -140,3 +140,24 @@ def test_levels_default_by_size(bc):
 def test_levels_invalid_count(bc):
     import bellman_cuda as bcm
     assert bc.lib.msm_b200_set_affine_levels(5) == bcm.BC_ERROR_INVALID_VALUE
+
+
+def test_levels_chunked_host_scalars(bc, oracle):
+    """Host-resident (pageable) scalars are processed in chunks, each running
+    its own levels over its own sorted entries into the chunk's buckets."""
+    n = 1 << 20
+    scalars, k = synth.workload("uniform", n, 977)
+    kd = bc.to_device(k)
+    bd = bc.malloc(n * 64)
+    bc.generator_multiples(kd, bd, n, bc.stream_handle)
+    bc.stream_synchronize(bc.stream_handle)
+    bc.free(kd)
+    res = np.zeros((254, 24), np.uint32)
+    bc.set_affine_levels(2)
+    try:
+        assert bc.msm_execute_async(bc.pool_handle, bc.stream_handle, bd, np.ascontiguousarray(scalars), res, 20) == 0
+        bc.stream_synchronize(bc.stream_handle)
+    finally:
+        bc.set_affine_levels(-1)
+        bc.free(bd)
+    assert oracle.horner(res) == oracle.msm_checksum(k, scalars)
