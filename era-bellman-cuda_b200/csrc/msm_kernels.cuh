@@ -50,9 +50,10 @@ constexpr unsigned SORT_TILE = SORT_THREADS * SORT_ITEMS;
 // Resident scatter blocks per SM (4 caps registers at 64, with a few bytes of
 // spills): at 2^22 the sort stage took 1.067 ms at 3 blocks, 1.012 at 4.
 // Resident blocks per SM the reduction kernels are compiled for (1: as many
-// as their registers allow).  reduce_groups_kernel at 3 (168 registers, some
-// spills, instead of 206 registers and 2 blocks): reduction 0.695 -> 0.664 ms
-// at 2^22; reduce_level_kernel at 4 measured no better.
+// as their registers allow).  reduce_groups_kernel at 3 (168 registers, 140
+// bytes of spills, instead of 206 registers and 2 blocks): reduction stage at
+// 2^22 0.695 -> 0.664 ms with groups of 8 slots, 0.692 -> 0.637 ms with the
+// groups of 4 it uses there now; reduce_level_kernel at 4 measured no better.
 #ifndef REDUCE_GROUPS_MIN_BLOCKS
 #define REDUCE_GROUPS_MIN_BLOCKS 3
 #endif
