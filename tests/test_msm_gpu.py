@@ -488,3 +488,29 @@ def test_profiled_counts(gpu, oracle, dist):
     assert 0 < prof.nonempty_buckets <= windows << (c - 1)
     assert prof.madds == prof.nonzero_entries - prof.nonempty_buckets - prof.heads
     assert oracle.horner(res) == oracle.msm_checksum(k, scalars)
+
+
+@pytest.mark.parametrize("smem", ["pinned", "pageable"])
+def test_chunked_host_inputs_ragged(gpu, oracle, smem):
+    """Host-resident scalars of a length that is neither a power of two nor a
+    multiple of the sort tile (3,000,017 points) through the any-length entry
+    point: chunk boundaries fall mid-tile, the last chunk is ragged."""
+    n = 3_000_017
+    scalars, k = synth.workload("uniform", n, 611)
+    bd, _ = generated_bases(gpu, k)
+    rd = gpu.bc.malloc(254 * 96)
+    pinned = None
+    if smem == "pinned":
+        hs, pinned = gpu.bc.pinned_array(scalars.shape)
+        hs[...] = scalars
+        src = pinned
+    else:
+        src = np.ascontiguousarray(scalars)
+    assert gpu.bc.msm_any(gpu.pool, gpu.stream, bd, src, rd, n, 0) == 0
+    gpu.bc.stream_synchronize(gpu.stream)
+    res = gpu.bc.from_device(rd, (254, 24))
+    for p in (bd, rd):
+        gpu.bc.free(p)
+    if pinned is not None:
+        gpu.bc.free_host(pinned)
+    assert oracle.horner(res) == oracle.msm_checksum(k, scalars)
