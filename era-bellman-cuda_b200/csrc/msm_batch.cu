@@ -11,9 +11,12 @@
 //   digits       every point of every instance, W(c_k) signed digits each, into
 //                its instance's segment of W(c_k) windows of n_k rounded up
 //                to whole sort tiles (the padding holds zero digits), with the
-//                first radix pass's tile counts
+//                first radix pass's tile counts and every later pass's digit
+//                totals per segment
 //   sort         segmented LSD radix sort, tile list over all segments; the
-//                first pass drops zero digits (counted per segment)
+//                first pass (scan + scatter) drops zero digits (counted per
+//                segment), every later pass is one look-back kernel whose
+//                tiles are handed out interleaved over the segments
 //   accumulate   the nonzero entries of all segments split into equal ranges,
 //                one per thread: the (instance, bucket-range) work list
 //   merge heads  as in the plain pipeline
@@ -103,18 +106,25 @@ __global__ void __launch_bounds__(128) window_multiples_kernel(const affine *__r
 // the entries of window w of this point tile are exactly sort tile w *
 // point_tiles + p of the segment, so these are the first radix pass's tile
 // counts, written for batch_sort_scan_kernel (no histogram kernel for that
-// pass).  Zero digits (padding included) are added to zeros[k].
+// pass).  Zero digits (padding included) are added to zeros[k].  The block
+// also counts its nonzero keys per radix digit of every later pass and adds
+// them to the instance's digit totals of that pass, later_totals[(pass - 1)
+// * instances + k][digit], which the look-back passes need up front.
 __global__ void __launch_bounds__(SORT_THREADS) batch_digits_histogram_kernel(const batch_instance *__restrict__ inst,
                                                                               const unsigned *__restrict__ ptile_seg, const batch_io *__restrict__ io,
                                                                               uint32_t *__restrict__ keys, uint32_t *__restrict__ vals,
-                                                                              uint32_t *__restrict__ counts, uint32_t *__restrict__ zeros) {
-  extern __shared__ uint32_t s_hist[]; // [windows][SORT_RADIX], then the zero-digit count
+                                                                              uint32_t *__restrict__ counts, uint32_t *__restrict__ zeros,
+                                                                              unsigned instances, unsigned later_passes,
+                                                                              uint32_t *__restrict__ later_totals) {
+  // [windows][SORT_RADIX] first-pass counters, [later_passes][SORT_RADIX], then the zero-digit count
+  extern __shared__ uint32_t s_hist[];
   const unsigned k = ptile_seg[blockIdx.x];
   const batch_instance d = inst[k];
   const unsigned tile = blockIdx.x - d.ptile_base, windows = d.windows;
-  const unsigned counters = windows * SORT_RADIX;
-  uint32_t *zero_digits = s_hist + counters;
-  for (unsigned q = threadIdx.x; q <= counters; q += blockDim.x)
+  const unsigned counters = windows * SORT_RADIX, later = later_passes * SORT_RADIX;
+  uint32_t *s_later = s_hist + counters;
+  uint32_t *zero_digits = s_later + later;
+  for (unsigned q = threadIdx.x; q <= counters + later; q += blockDim.x)
     s_hist[q] = 0;
   __syncthreads();
   const fe *scalars = io[k].scalars;
@@ -138,10 +148,13 @@ __global__ void __launch_bounds__(SORT_THREADS) batch_digits_histogram_kernel(co
           const uint32_t key = digit_key(magnitude);
           keys[out] = key;
           vals[out] = (w * d.stride + i) | (negative << 31);
-          if (magnitude)
+          if (magnitude) {
             atomicAdd(&s_hist[w * SORT_RADIX + (key & (SORT_RADIX - 1))], 1u);
-          else
+            for (unsigned p = 0; p < later_passes; p++)
+              atomicAdd(&s_later[p * SORT_RADIX + ((key >> ((p + 1) * SORT_RADIX_BITS)) & (SORT_RADIX - 1))], 1u);
+          } else {
             zero_count++;
+          }
         });
       } else {
         for (unsigned w = 0; w < windows; w++) {
@@ -167,27 +180,18 @@ __global__ void __launch_bounds__(SORT_THREADS) batch_digits_histogram_kernel(co
     const unsigned w = q / SORT_RADIX, dg = q % SORT_RADIX;
     counts[(size_t)d.tile_base * SORT_RADIX + (size_t)dg * d.tiles + w * d.point_tiles + tile] = s_hist[q];
   }
+  for (unsigned q = threadIdx.x; q < later; q += blockDim.x) // q = (pass - 1) * 256 + digit
+    if (s_later[q])
+      atomicAdd(&later_totals[((size_t)(q / SORT_RADIX) * instances + k) * SORT_RADIX + q % SORT_RADIX], s_later[q]);
   if (threadIdx.x == 0 && *zero_digits)
     atomicAdd(&zeros[k], *zero_digits);
 }
 
 // Dynamic shared memory of batch_digits_histogram_kernel for an instance of
-// window width c: a counter per (window, digit) and the zero-digit count.
-static size_t batch_digit_smem(unsigned c) { return ((size_t)windows_for(c) * SORT_RADIX + 1) * 4; }
-
-// A later radix pass's tile counts of every segment's nonzero entries
-// [entry_offset + zeros[k], entry_offset + entries), where the first pass
-// put them.
-__global__ void __launch_bounds__(SORT_THREADS) batch_sort_histogram_kernel(const uint32_t *__restrict__ keys, const batch_instance *__restrict__ inst,
-                                                                            const unsigned *__restrict__ tile_seg, unsigned shift,
-                                                                            uint32_t *__restrict__ counts, const uint32_t *__restrict__ zeros) {
-  const unsigned t = blockIdx.x;
-  const unsigned k = tile_seg[t];
-  const batch_instance d = inst[k];
-  const unsigned skip = zeros[k], live = d.entries - skip;
-  const unsigned local = t - d.tile_base, base = local * SORT_TILE;
-  sort_histogram_tile<false>(keys + d.entry_offset + skip, base, base < live ? min(SORT_TILE, live - base) : 0, shift,
-                             counts + (size_t)d.tile_base * SORT_RADIX + local, d.tiles, nullptr);
+// window width c: a counter per (window, digit), per (later pass, digit) and
+// the zero-digit count.
+static size_t batch_digit_smem(unsigned c, unsigned later_passes) {
+  return ((size_t)(windows_for(c) + later_passes) * SORT_RADIX + 1) * 4;
 }
 
 // one warp per (segment, digit) row
@@ -200,30 +204,49 @@ __global__ void __launch_bounds__(256) batch_sort_scan_kernel(uint32_t *counts, 
   sort_scan_row(counts + (size_t)d.tile_base * SORT_RADIX + (size_t)(row % SORT_RADIX) * d.tiles, d.tiles, totals + row);
 }
 
-template <bool STABLE>
-__global__ void __launch_bounds__(SORT_THREADS, SORT_SCATTER_MIN_BLOCKS) batch_sort_scatter_kernel(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
-                                                                          uint32_t *__restrict__ keys_out, uint32_t *__restrict__ vals_out,
-                                                                          const batch_instance *__restrict__ inst,
-                                                                          const unsigned *__restrict__ tile_seg, unsigned shift,
-                                                                          const uint32_t *__restrict__ counts, const uint32_t *__restrict__ totals,
-                                                                          const uint32_t *__restrict__ zeros) {
+// The first radix pass (drops zero digits; tile offsets from the scan).
+__global__ void __launch_bounds__(SORT_THREADS, SORT_SCATTER_MIN_BLOCKS) batch_sort_scatter_first_kernel(
+    const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in, uint32_t *__restrict__ keys_out, uint32_t *__restrict__ vals_out,
+    const batch_instance *__restrict__ inst, const unsigned *__restrict__ tile_seg, const uint32_t *__restrict__ counts,
+    const uint32_t *__restrict__ totals, const uint32_t *__restrict__ zeros) {
   const unsigned t = blockIdx.x;
   const unsigned k = tile_seg[t];
   const batch_instance d = inst[k];
   const unsigned local = t - d.tile_base, base = local * SORT_TILE;
   const unsigned skip = zeros[k];
   const uint32_t *tile_counts = counts + (size_t)d.tile_base * SORT_RADIX + local;
-  if (STABLE) {
-    const unsigned live = d.entries - skip;
-    if (base >= live)
-      return;
-    const size_t seg = d.entry_offset + skip;
-    sort_scatter_tile<true, false>(keys_in, vals_in, keys_out, vals_out, seg, seg, base, min(SORT_TILE, live - base), shift, tile_counts, d.tiles,
-                                   totals + (size_t)k * SORT_RADIX);
-  } else {
-    sort_scatter_tile<false, true>(keys_in, vals_in, keys_out, vals_out, d.entry_offset, d.entry_offset + skip, base,
-                                   min(SORT_TILE, d.entries - base), shift, tile_counts, d.tiles, totals + (size_t)k * SORT_RADIX);
-  }
+  sort_scatter_tile<false, true>(keys_in, vals_in, keys_out, vals_out, d.entry_offset, d.entry_offset + skip, base,
+                                 min(SORT_TILE, d.entries - base), 0, tile_counts, d.tiles, totals + (size_t)k * SORT_RADIX);
+}
+
+// A later radix pass in one kernel, positions by decoupled look-back
+// (lookback_tile) over the tiles of each instance's segment.  Blocks take
+// tickets from *tile_ctr, and ticket q sorts tile tile_order[q]: the
+// instances' tiles interleaved (every instance's local tile j before any
+// instance's tile j + 1), so the tiles in flight spread over the instances
+// and a tile's look-back walks over few aggregates of its own segment; its
+// predecessors took their tickets earlier and are resident.  agg and incl
+// hold 256 counts per global tile, flags one word per global tile (this
+// pass's, zero at launch); totals: the instances' digit totals of this pass.
+__global__ void __launch_bounds__(SORT_THREADS, SORT_SCATTER_MIN_BLOCKS) batch_lookback_kernel(
+    const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in, uint32_t *__restrict__ keys_out, uint32_t *__restrict__ vals_out,
+    const batch_instance *__restrict__ inst, const unsigned *__restrict__ tile_seg, const unsigned *__restrict__ tile_order, unsigned shift,
+    uint32_t *flags, uint32_t *agg, uint32_t *incl, const uint32_t *__restrict__ totals, const uint32_t *__restrict__ zeros, unsigned *tile_ctr,
+    unsigned *error) {
+  __shared__ unsigned s_ticket;
+  if (threadIdx.x == 0)
+    s_ticket = atomicAdd(tile_ctr, 1u);
+  __syncthreads();
+  const unsigned t = tile_order[s_ticket];
+  const unsigned k = tile_seg[t];
+  const batch_instance d = inst[k];
+  const unsigned local = t - d.tile_base, base = local * SORT_TILE;
+  const unsigned skip = zeros[k], live = d.entries - skip;
+  if (base >= live) // no later tile of this segment holds entries either, so none waits for this one
+    return;
+  const size_t rows = (size_t)d.tile_base * SORT_RADIX;
+  lookback_tile(keys_in, vals_in, keys_out, vals_out, d.entry_offset + skip, local, min(SORT_TILE, live - base), shift, flags + d.tile_base,
+                agg + rows, incl + rows, totals + (size_t)k * SORT_RADIX, error);
 }
 
 // The batch's segments for accumulate_ranges: one per instance.
@@ -497,7 +520,6 @@ cudaError_t make_batch_plan(batch_plan &b, const base_table_impl *table, const u
     b.total_entries += d.entries;
     b.total_tiles += d.tiles;
     b.total_point_tiles += d.point_tiles;
-    b.digit_smem = std::max(b.digit_smem, batch_digit_smem(c));
     points += n;
     max_c = std::max(max_c, c);
     by_c[c].push_back(k);
@@ -506,6 +528,8 @@ cudaError_t make_batch_plan(batch_plan &b, const base_table_impl *table, const u
     return cudaErrorInvalidValue;
   b.total_points = (unsigned)points;
   b.sort_passes = (max_c - 1 + SORT_RADIX_BITS - 1) / SORT_RADIX_BITS; // keys take c - 1 bits
+  for (const batch_instance &d : b.inst)
+    b.digit_smem = std::max(b.digit_smem, batch_digit_smem(d.c, b.sort_passes - 1));
   for (auto &kv : by_c) {
     batch_group g;
     g.c = kv.first;
@@ -532,9 +556,21 @@ cudaError_t make_batch_plan(batch_plan &b, const base_table_impl *table, const u
     b.keys[i] = take(b.total_entries * 4);
     b.vals[i] = take(b.total_entries * 4);
   }
+  // the first pass's tile counts, reused by the later passes as the tiles'
+  // look-back aggregates; the look-back inclusive counts
   b.counts = take((size_t)b.total_tiles * SORT_RADIX * 4);
+  b.incl = b.sort_passes > 1 ? take((size_t)b.total_tiles * SORT_RADIX * 4) : 0;
   b.totals = take((size_t)instances * SORT_RADIX * 4);
-  b.zeros = take((size_t)instances * 4);
+  // cleared every execution: zero digits per instance, the later passes'
+  // digit totals per instance, their look-back flags per tile, a tile ticket
+  // counter per later pass and the look-back error word
+  const unsigned later = b.sort_passes - 1;
+  b.zeros = take(((size_t)instances + (size_t)later * instances * SORT_RADIX + (size_t)later * b.total_tiles + later + 1) * 4);
+  b.later_totals = b.zeros + (size_t)instances * 4;
+  b.lookback_flags = b.later_totals + (size_t)later * instances * SORT_RADIX * 4;
+  b.sort_ctrs = b.lookback_flags + (size_t)later * b.total_tiles * 4;
+  b.sort_error = b.sort_ctrs + (size_t)later * 4;
+  b.sort_clear_bytes = b.sort_error + 4 - b.zeros;
   b.buckets = take((size_t)b.slots * sizeof(xyzz));
   b.flags = take(b.slots);
   for (int i = 0; i < 2; i++) {
@@ -552,6 +588,7 @@ cudaError_t make_batch_plan(batch_plan &b, const base_table_impl *table, const u
   b.descriptors = off;
   b.inst_dev = take(instances * sizeof(batch_instance));
   b.tile_seg_dev = take((size_t)b.total_tiles * 4);
+  b.tile_order_dev = take((size_t)b.total_tiles * 4);
   b.ptile_seg_dev = take((size_t)b.total_point_tiles * 4);
   for (batch_group &g : b.groups)
     g.members_dev = take(g.members.size() * 4);
@@ -566,10 +603,19 @@ std::vector<uint8_t> descriptor_image(const batch_plan &b) {
   put(b.inst_dev, b.inst.data(), b.instances * sizeof(batch_instance));
   unsigned *tile_seg = reinterpret_cast<unsigned *>(img.data() + (b.tile_seg_dev - b.descriptors));
   unsigned *ptile_seg = reinterpret_cast<unsigned *>(img.data() + (b.ptile_seg_dev - b.descriptors));
+  unsigned most = 0;
   for (unsigned k = 0; k < b.instances; k++) {
     std::fill(tile_seg + b.inst[k].tile_base, tile_seg + b.inst[k].tile_base + b.inst[k].tiles, k);
     std::fill(ptile_seg + b.inst[k].ptile_base, ptile_seg + b.inst[k].ptile_base + b.inst[k].point_tiles, k);
+    most = std::max(most, b.inst[k].tiles);
   }
+  // the look-back passes' ticket order: local tile j of every instance before local tile j + 1 of any
+  unsigned *tile_order = reinterpret_cast<unsigned *>(img.data() + (b.tile_order_dev - b.descriptors));
+  unsigned q = 0;
+  for (unsigned j = 0; j < most; j++)
+    for (unsigned k = 0; k < b.instances; k++)
+      if (j < b.inst[k].tiles)
+        tile_order[q++] = b.inst[k].tile_base + j;
   for (const batch_group &g : b.groups)
     put(g.members_dev, g.members.data(), g.members.size() * 4);
   return img;
@@ -595,31 +641,33 @@ cudaError_t enqueue_batch(const batch_plan &b, uint8_t *scratch, cudaStream_t s,
   xyzz *hp[2] = {reinterpret_cast<xyzz *>(at(b.hp[0])), reinterpret_cast<xyzz *>(at(b.hp[1]))};
 
   CHECK(cudaMemsetAsync(flags, 0, b.slots, s));
-  CHECK(cudaMemsetAsync(zeros, 0, b.instances * sizeof(uint32_t), s));
-  // digits, with the first pass's counts per sort tile
+  CHECK(cudaMemsetAsync(zeros, 0, b.sort_clear_bytes, s));
+  const unsigned later = b.sort_passes - 1;
+  uint32_t *later_totals = reinterpret_cast<uint32_t *>(at(b.later_totals));
+  // digits, with the first pass's counts per sort tile and the later passes' digit totals
   batch_digits_histogram_kernel<<<b.total_point_tiles, SORT_THREADS, b.digit_smem, s>>>(
-      inst, reinterpret_cast<const unsigned *>(at(b.ptile_seg_dev)), io, keys[0], vals[0], counts, zeros);
+      inst, reinterpret_cast<const unsigned *>(at(b.ptile_seg_dev)), io, keys[0], vals[0], counts, zeros, b.instances, later, later_totals);
   CHECK(cudaGetLastError());
   launched++;
-  int cur = 0;
+  // the first pass: tile offsets and digit totals by one scan, then the scatter (drops zero digits)
   const unsigned rows = b.instances * SORT_RADIX;
-  for (unsigned pass = 0; pass < b.sort_passes; pass++) {
-    const unsigned shift = pass * SORT_RADIX_BITS;
-    if (pass > 0) {
-      batch_sort_histogram_kernel<<<b.total_tiles, SORT_THREADS, 0, s>>>(keys[cur], inst, tile_seg, shift, counts, zeros);
-      CHECK(cudaGetLastError());
-      launched++;
-    }
-    batch_sort_scan_kernel<<<(rows * 32 + 255) / 256, 256, 0, s>>>(counts, inst, rows, totals);
+  batch_sort_scan_kernel<<<(rows * 32 + 255) / 256, 256, 0, s>>>(counts, inst, rows, totals);
+  CHECK(cudaGetLastError());
+  batch_sort_scatter_first_kernel<<<b.total_tiles, SORT_THREADS, 0, s>>>(keys[0], vals[0], keys[1], vals[1], inst, tile_seg, counts, totals, zeros);
+  CHECK(cudaGetLastError());
+  launched += 2;
+  int cur = 1;
+  // later passes: one look-back kernel each
+  const unsigned *tile_order = reinterpret_cast<const unsigned *>(at(b.tile_order_dev));
+  uint32_t *lookback_flags = reinterpret_cast<uint32_t *>(at(b.lookback_flags)), *incl = reinterpret_cast<uint32_t *>(at(b.incl));
+  unsigned *sort_ctrs = reinterpret_cast<unsigned *>(at(b.sort_ctrs)), *sort_error = reinterpret_cast<unsigned *>(at(b.sort_error));
+  for (unsigned pass = 1; pass < b.sort_passes; pass++) {
+    batch_lookback_kernel<<<b.total_tiles, SORT_THREADS, 0, s>>>(
+        keys[cur], vals[cur], keys[cur ^ 1], vals[cur ^ 1], inst, tile_seg, tile_order, pass * SORT_RADIX_BITS,
+        lookback_flags + (size_t)(pass - 1) * b.total_tiles, counts, incl, later_totals + (size_t)(pass - 1) * b.instances * SORT_RADIX, zeros,
+        sort_ctrs + pass - 1, sort_error);
     CHECK(cudaGetLastError());
-    if (pass == 0)
-      batch_sort_scatter_kernel<false><<<b.total_tiles, SORT_THREADS, 0, s>>>(keys[cur], vals[cur], keys[cur ^ 1], vals[cur ^ 1], inst, tile_seg,
-                                                                             shift, counts, totals, zeros);
-    else
-      batch_sort_scatter_kernel<true><<<b.total_tiles, SORT_THREADS, 0, s>>>(keys[cur], vals[cur], keys[cur ^ 1], vals[cur ^ 1], inst, tile_seg,
-                                                                            shift, counts, totals, zeros);
-    CHECK(cudaGetLastError());
-    launched += 2;
+    launched++;
     cur ^= 1;
   }
   unsigned *work = reinterpret_cast<unsigned *>(at(b.work));
@@ -774,9 +822,10 @@ cudaError_t batch_execute(batch_impl *bi, const void *const *scalars, void *cons
 
 cudaError_t batch_set_up() {
   CHECK(cudaFuncSetAttribute(batch_accumulate_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, 50));
-  size_t digit_smem = 0; // the widest instance any batch can hold
+  size_t digit_smem = 0; // the widest instance any batch can hold, with the most later passes
+  const unsigned most_later = (MAX_TABLE_BITS - 1 + SORT_RADIX_BITS - 1) / SORT_RADIX_BITS - 1;
   for (unsigned c = 2; c <= MAX_TABLE_BITS; c++)
-    digit_smem = std::max(digit_smem, batch_digit_smem(c));
+    digit_smem = std::max(digit_smem, batch_digit_smem(c, most_later));
   CHECK(cudaFuncSetAttribute(batch_digits_histogram_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)digit_smem));
   return cudaSuccess;
 }
