@@ -143,7 +143,7 @@ static unsigned reduction_log_m(unsigned c) { return c <= 14 ? 1 : c == 15 ? 3 :
 
 // Groups of 2^log_m slots (at most the window's slots); the reduction's tree
 // and stream buffers hold G = 2^(log_b - log_m) entries per window.
-static void set_reduction_groups(plan &p, unsigned log_m) {
+void set_reduction_groups(plan &p, unsigned log_m) {
   p.log_m = std::min(log_m, p.log_b);
   p.log_g = p.log_b - p.log_m;
   p.groups = 1u << p.log_g;

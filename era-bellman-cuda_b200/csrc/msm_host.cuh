@@ -73,6 +73,8 @@ void set_affine_levels_override(int levels);
 // p with `levels` affine pairing levels (0 for inputs whose list positions
 // would not fit 31 bits), and the geometry of the levels and of the XYZZ pass after them
 void set_affine_levels(plan &p, unsigned levels);
+// the reduction's groups of 2^log_m bucket slots (capped at the window's slots)
+void set_reduction_groups(plan &p, unsigned log_m);
 unsigned accumulation_ranges(unsigned threads, unsigned long long entries, unsigned per_thread);
 plan make_plan(unsigned n, unsigned window_bits, int sms);
 size_t scratch_bytes(unsigned n, unsigned window_bits, bool copy_scalars, bool copy_bases, bool copy_results);
