@@ -38,6 +38,11 @@
 // never a field element below p), which later levels and the XYZZ pass skip.
 // Every stored coordinate is fully reduced, so equal x means equal points or
 // opposite ones, and no slope denominator is ever 0 mod p.
+//
+// The levels are off by default (msm_b200_set_affine_levels turns them on):
+// on a B200 each level's two passes over its list in memory, and the first
+// level's two random gathers of every base, cost more than the multiplies
+// they save (measurements with default_affine_levels in msm_host.cu).
 #pragma once
 
 #include "msm_device.cuh"
