@@ -142,3 +142,32 @@ def test_onesweep_model_sorts_each_window(trial):
         # equal full keys is whatever the first pass left (any order)
         assert [k for k, _ in got] == sorted(k for k, _ in nonzero)
         assert sorted(got) == sorted(nonzero)
+
+
+def batch_ticket_order(tiles):
+    """The batched look-back passes' ticket order (msm_batch.cu,
+    descriptor_image): instance k's local tile j is global tile base[k] + j,
+    and every instance's local tile j comes before any instance's tile j + 1."""
+    base, acc = [], 0
+    for t in tiles:
+        base.append(acc)
+        acc += t
+    order = []
+    for j in range(max(tiles, default=0)):
+        for k, t in enumerate(tiles):
+            if j < t:
+                order.append(base[k] + j)
+    return order, base
+
+
+@pytest.mark.parametrize("tiles", [[1], [5, 1, 3], [2000, 7, 0 + 1, 1300, 64], [3] * 64, [13312, 11000, 40, 1]])
+def test_batch_ticket_order(tiles):
+    """Every tile gets exactly one ticket, and a tile's predecessors in its
+    own segment (the only tiles its look-back waits for) hold earlier tickets,
+    so they are resident or finished whenever it waits."""
+    order, base = batch_ticket_order(tiles)
+    assert sorted(order) == list(range(sum(tiles)))
+    ticket = {t: q for q, t in enumerate(order)}
+    for k, n in enumerate(tiles):
+        for j in range(1, n):
+            assert ticket[base[k] + j - 1] < ticket[base[k] + j]
