@@ -183,7 +183,8 @@ plan make_plan(unsigned n, unsigned window_bits, int sms) {
 // two chunks 1:5 12.94 ms, 1:6 13.11 ms (chunk 1's copy outlasts chunk 0's
 // work), 1:4 level with 1:5, 1:3 slower; three chunks 1:4:16 13.13 ms.  With
 // the later accumulation-range and segment-alignment fixes, three chunks 1:5:25
-// still lose to two: 12.30 against 12.27 ms.
+// still lose to two: 12.30 against 12.27 ms; with the warp-scan head merge
+// and the current sort, 11.964 against 11.954 ms.
 // Folding by continuing the earlier chunks' buckets inside the accumulation
 // (no second bucket set, no fold kernel) measured slower: 13.02 against
 // 12.85 ms at 2^22, 25.2 against 23.4 ms at 2^23.  Reference counterpart: the
