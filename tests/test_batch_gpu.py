@@ -167,3 +167,28 @@ def test_batch_config3_full(lib, oracle):
         assert oracle.horner(res) == oracle.msm_checksum(k[:n], s), f"instance {j} (n={n}, {dist})"
     lib.bc.base_table_destroy(table)
     lib.bc.free(bd)
+
+
+def test_batch_many_instances_edge_scalars(lib, oracle, table16):
+    """The batch's limit of 256 instances: a 2^16-point instance beside 255
+    small ones (so the look-back passes' interleaved ticket order ends with
+    one segment alone), instances of all-zero scalars (no nonzero entry: every
+    later-pass tile of the segment returns at once), all ones (one heavy
+    bucket), r - 1, 2^253 and (r + 1) / 2."""
+    import numpy as np
+    import msm_helpers as H
+    k, _, table = table16
+    rng = np.random.Generator(np.random.PCG64(77))
+    lengths = [1 << 16] + [int(x) for x in rng.integers(1, 3000, size=255)]
+    fixed = {1: 0, 2: 1, 3: H.R - 1, 4: 1 << 253, 5: (H.R + 1) // 2}
+    work = []
+    for j, n in enumerate(lengths):
+        if j in fixed:
+            work.append(H.mont_scalar_array([fixed[j]] * n))
+        elif j % 2:
+            work.append(synth.skewed_scalars(900 + j, n))
+        else:
+            work.append(synth.uniform_scalars(900 + j, n))
+    results = lib.run_batch(table, work)
+    for j, (n, s, res) in enumerate(zip(lengths, work, results)):
+        assert oracle.horner(res) == oracle.msm_checksum(k[:n], s), f"instance {j} (n={n})"
