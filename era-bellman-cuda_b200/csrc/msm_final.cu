@@ -15,6 +15,7 @@
 // 254 squarings).
 #include "bellman-cuda-b200.h"
 #include "msm_device.cuh"
+#include "msm_group4.cuh"
 #include "pointer_access.h"
 
 #include <cuda_runtime.h>
@@ -22,50 +23,6 @@
 namespace msm_b200 {
 
 constexpr unsigned FINAL_THREADS = 128; // threads t < 127 start from results 2t, 2t + 1
-
-__device__ __forceinline__ fe shfl_fe(const fe &v, unsigned src) {
-  fe r;
-#pragma unroll
-  for (int k = 0; k < 8; k++)
-    r.l[k] = __shfl_sync(0xffffffffu, v.l[k], src);
-  return r;
-}
-
-__device__ __forceinline__ fe select_fe(bool c, const fe &a, const fe &b) {
-  fe r;
-#pragma unroll
-  for (int k = 0; k < 8; k++)
-    r.l[k] = c ? a.l[k] : b.l[k];
-  return r;
-}
-
-// One XYZZ doubling (dbl-2008-s-1, the formula of curve::dbl) by a group of
-// four lanes: lanes 4g..4g+3 hold the same point and all return its double.
-// The formula's independent products run on different lanes of the group in
-// three rounds -- X^2 | (2Y)^2;  M^2 | X V | U V | V ZZ;  M (S - X3) - W Y |
-// W ZZZ -- and shuffles share the results, so one doubling costs three
-// dependent products instead of ten.  Every lane runs the same instructions
-// on its own operands (no divergence), so every lane of the warp must call
-// it.  Infinity (ZZ = 0) maps to a point with ZZ = 0, i.e. to infinity.
-__device__ __forceinline__ xyzz dbl_group4(const xyzz &p) {
-  const unsigned lane = threadIdx.x & 31, role = lane & 3, base = lane & ~3u;
-  const fe U = fq::dbl(p.y);
-  const fe r1 = fq::sqr(select_fe(role == 0, p.x, U));
-  const fe X2 = shfl_fe(r1, base), V = shfl_fe(r1, base + 1);
-  const fe M = fq::add(fq::dbl(X2), X2);
-  const fe a2 = role == 0 ? M : role == 1 ? p.x : role == 2 ? U : V;
-  const fe b2 = role == 0 ? M : role == 3 ? p.zz : V;
-  const fe r2 = fq::mul(a2, b2);
-  const fe M2 = shfl_fe(r2, base), S = shfl_fe(r2, base + 1), W = shfl_fe(r2, base + 2), ZZ3 = shfl_fe(r2, base + 3);
-  xyzz r;
-  r.x = fq::sub(M2, fq::dbl(S));
-  const bool lead = role == 0;
-  const fe r3 = fq::mul_sub_mul(lead ? M : W, lead ? fq::sub(S, r.x) : p.zzz, lead ? W : fq::zero(), lead ? p.y : fq::zero());
-  r.y = shfl_fe(r3, base);
-  r.zzz = shfl_fe(r3, base + 1);
-  r.zz = ZZ3;
-  return r;
-}
 
 __global__ void __launch_bounds__(FINAL_THREADS) final_sum_kernel(const jacobian *__restrict__ results, msm_b200_affine_point *point) {
   __shared__ xyzz part[FINAL_THREADS]; // part[t]: the sum of the bits starting at 2t (weights relative to 2^2t)

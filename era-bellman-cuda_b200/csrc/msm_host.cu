@@ -567,16 +567,28 @@ static cudaError_t enqueue_accumulation(const plan &p, const fe *scalars, const 
 // of 96 slower (reduction 0.695 -> 0.815 ms).
 cudaError_t enqueue_window_sums(const plan &p, const xyzz *buckets, const uint8_t *flags, xyzz *const tree[2], xyzz *const streams[2],
                                 cudaStream_t stream, unsigned &launched) {
+  // Launches with fewer jobs than one block of ACC_THREADS per SM run a group
+  // of four lanes per job (msm_group4.cuh): there each job's chain of
+  // additions is the launch's latency, and four times the threads still fit.
+  const unsigned small = p.sms * ACC_THREADS;
+  auto blocks = [](unsigned long long threads) { return (unsigned)((threads + ACC_THREADS - 1) / ACC_THREADS); };
   const unsigned group_threads = p.windows << p.log_g;
-  reduce_groups_kernel<<<(group_threads + ACC_THREADS - 1) / ACC_THREADS, ACC_THREADS, 0, stream>>>(buckets, flags, p.windows, p.log_b,
-                                                                                                     p.log_m, tree[0], streams[0]);
+  if (group_threads <= small)
+    reduce_groups_group4_kernel<<<blocks(4ull * group_threads), ACC_THREADS, 0, stream>>>(buckets, flags, p.windows, p.log_b, p.log_m, tree[0],
+                                                                                          streams[0]);
+  else
+    reduce_groups_kernel<<<blocks(group_threads), ACC_THREADS, 0, stream>>>(buckets, flags, p.windows, p.log_b, p.log_m, tree[0], streams[0]);
   CHECK(cudaGetLastError());
   launched++;
   for (unsigned level = 0; level < p.log_g; level++) {
     const unsigned threads = p.windows * (level + 2) * ((1u << p.log_g) >> (level + 1));
     const int in = level & 1;
-    reduce_level_kernel<<<(threads + ACC_THREADS - 1) / ACC_THREADS, ACC_THREADS, 0, stream>>>(tree[in], tree[in ^ 1], streams[in], streams[in ^ 1],
-                                                                                                p.windows, p.log_g, level);
+    if (threads <= small)
+      reduce_level_group4_kernel<<<blocks(4ull * threads), ACC_THREADS, 0, stream>>>(tree[in], tree[in ^ 1], streams[in], streams[in ^ 1],
+                                                                                      p.windows, p.log_g, level);
+    else
+      reduce_level_kernel<<<blocks(threads), ACC_THREADS, 0, stream>>>(tree[in], tree[in ^ 1], streams[in], streams[in ^ 1], p.windows, p.log_g,
+                                                                       level);
     CHECK(cudaGetLastError());
     launched++;
   }

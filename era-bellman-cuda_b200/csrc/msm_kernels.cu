@@ -1,6 +1,7 @@
 // Device kernels of the Pippenger MSM pipeline; see msm_kernels.cuh for the
 // overall data flow.
 #include "msm_affine.cuh"
+#include "msm_group4.cuh"
 
 namespace msm_b200 {
 
@@ -363,16 +364,6 @@ __global__ void __launch_bounds__(ACC_THREADS, ACC_MIN_BLOCKS) accumulate_list_k
 // ---------------------------------------------------------------------------
 // 5. fold head partial sums into their buckets
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ xyzz shfl_up_xyzz(const xyzz &v, unsigned delta) {
-  xyzz r;
-  const uint32_t *a = reinterpret_cast<const uint32_t *>(&v);
-  uint32_t *b = reinterpret_cast<uint32_t *>(&r);
-#pragma unroll
-  for (int i = 0; i < 32; i++)
-    b[i] = __shfl_up_sync(0xffffffffu, a[i], delta);
-  return r;
-}
-
 // Warp w takes heads [32 w, 32 w + 32): a segmented inclusive scan over the
 // lanes (Kogge-Stone, five shuffle steps; the heads of one bucket are
 // contiguous, so equal buckets at distance d mean one segment in between)
@@ -492,6 +483,73 @@ __global__ void __launch_bounds__(ACC_THREADS, REDUCE_LEVEL_MIN_BLOCKS) reduce_l
     store_xyzz(s_out + sbase + stream_offset(log_g, level + 1) + i, b);
     if (level + 1 < log_g)
       store_xyzz(t_out + w * g + i, curve::add(a, b));
+  }
+}
+
+// reduce_groups_kernel and reduce_level_kernel with one group of four lanes
+// per thread of theirs (msm_group4.cuh), for launches too small to fill the
+// GPU, where each addition's issue time is the launch's latency.  Groups past
+// the end redo the first job and write nothing; whole warps past the end
+// leave.
+__global__ void __launch_bounds__(ACC_THREADS) reduce_groups_group4_kernel(const xyzz *__restrict__ buckets, const uint8_t *__restrict__ flags,
+                                                                           unsigned windows, unsigned log_b, unsigned log_m,
+                                                                           xyzz *__restrict__ run_out, xyzz *__restrict__ streams) {
+  const unsigned log_g = log_b - log_m;
+  const unsigned total = windows << log_g;
+  const unsigned t = blockIdx.x * blockDim.x + threadIdx.x, role = threadIdx.x & 3;
+  if ((t & ~31u) / 4 >= total)
+    return;
+  const bool active = t / 4 < total;
+  const unsigned gid = active ? t / 4 : 0;
+  const unsigned w = gid >> log_g, g = gid & ((1u << log_g) - 1);
+  const unsigned base = (w << log_b) + (g << log_m);
+  xyzz run = curve::infinity(), acc = curve::infinity();
+  for (unsigned i = (1u << log_m) - 1; i >= 1; i--) {
+    const xyzz x = flags[base + i] ? load_xyzz(buckets + base + i) : curve::infinity();
+    run = add_group4(run, x);
+    acc = add_group4(acc, run);
+  }
+  const xyzz x0 = g > 0 && flags[base] ? load_xyzz(buckets + base) : curve::infinity();
+  run = add_group4(run, x0);
+  if (active && role == 0) {
+    store_xyzz(run_out + gid, run);
+    store_xyzz(streams + (size_t)w * stream_stride(log_g) + stream_offset(log_g, 0) + g, acc);
+  }
+}
+
+__global__ void __launch_bounds__(ACC_THREADS) reduce_level_group4_kernel(const xyzz *__restrict__ t_in, xyzz *__restrict__ t_out,
+                                                                          const xyzz *__restrict__ s_in, xyzz *__restrict__ s_out, unsigned windows,
+                                                                          unsigned log_g, unsigned level) {
+  const unsigned half = (1u << log_g) >> (level + 1);
+  const unsigned jobs = level + 2; // streams 0..level, then the tree
+  const unsigned total = windows * jobs * half;
+  const unsigned t = blockIdx.x * blockDim.x + threadIdx.x, role = threadIdx.x & 3;
+  if ((t & ~31u) / 4 >= total)
+    return;
+  const bool active = t / 4 < total;
+  const unsigned gid = active ? t / 4 : 0;
+  const unsigned w = gid / (jobs * half), r = gid % (jobs * half);
+  const unsigned job = r / half, i = r % half;
+  const size_t g = (size_t)1 << log_g;
+  const size_t sbase = (size_t)w * stream_stride(log_g);
+  xyzz a, b;
+  if (job <= level) {
+    const size_t o = sbase + stream_offset(log_g, job);
+    a = load_xyzz(s_in + o + 2 * i);
+    b = load_xyzz(s_in + o + 2 * i + 1);
+  } else {
+    a = load_xyzz(t_in + w * g + 2 * i);
+    b = load_xyzz(t_in + w * g + 2 * i + 1);
+  }
+  const xyzz sum = add_group4(a, b);
+  if (!active || role != 0)
+    return;
+  if (job <= level) {
+    store_xyzz(s_out + sbase + stream_offset(log_g, job) + i, sum);
+  } else {
+    store_xyzz(s_out + sbase + stream_offset(log_g, level + 1) + i, b);
+    if (level + 1 < log_g)
+      store_xyzz(t_out + w * g + i, sum);
   }
 }
 

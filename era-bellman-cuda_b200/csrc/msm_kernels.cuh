@@ -185,7 +185,10 @@ __global__ void accumulate_list_kernel(const uint32_t *__restrict__ list_buckets
 // ---------------------------------------------------------------------------
 // 5. heads
 // ---------------------------------------------------------------------------
-// 32 heads per warp; one output head per warp (hb_out[w], INVALID_BUCKET if none)
+// 32 heads per warp; one output head per warp (hb_out[w], INVALID_BUCKET if
+// none).  A version with 8 heads per warp and 4-lane additions
+// (msm_group4.cuh) measured slower: 0.089 -> 0.123 ms at 2^12, 0.081 ->
+// 0.136 ms at 2^22 (more levels, heavier kernel).
 constexpr unsigned MERGE_HEADS_PER_WARP = 32;
 __global__ void merge_heads_kernel(const uint32_t *__restrict__ hb_in, const xyzz *__restrict__ hp_in, unsigned n_in, xyzz *__restrict__ buckets,
                                    uint32_t *__restrict__ hb_out, xyzz *__restrict__ hp_out);
@@ -202,6 +205,11 @@ __global__ void reduce_groups_kernel(const xyzz *__restrict__ buckets, const uin
 // one level of the tree and of every live stream (see msm_kernels.cu)
 __global__ void reduce_level_kernel(const xyzz *__restrict__ t_in, xyzz *__restrict__ t_out, const xyzz *__restrict__ s_in, xyzz *__restrict__ s_out,
                                     unsigned windows, unsigned log_g, unsigned level);
+// the same with a group of four lanes per thread of theirs (small launches)
+__global__ void reduce_groups_group4_kernel(const xyzz *__restrict__ buckets, const uint8_t *__restrict__ flags, unsigned windows, unsigned log_b,
+                                            unsigned log_m, xyzz *__restrict__ run, xyzz *__restrict__ streams);
+__global__ void reduce_level_group4_kernel(const xyzz *__restrict__ t_in, xyzz *__restrict__ t_out, const xyzz *__restrict__ s_in,
+                                           xyzz *__restrict__ s_out, unsigned windows, unsigned log_g, unsigned level);
 __global__ void gather_results_kernel(const xyzz *__restrict__ streams, const xyzz *__restrict__ buckets, const uint8_t *__restrict__ flags,
                                       unsigned windows, unsigned c, unsigned log_m, unsigned log_g, jacobian *__restrict__ results);
 
