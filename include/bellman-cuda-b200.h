@@ -237,7 +237,7 @@ bc_error msm_b200_execute_no_alloc_async(bc_stream stream, const void *bases, co
  *
  * Speed: this is not a faster Horner pass.  The sum needs 253 doublings in a
  * dependent chain whatever the order, and one GPU thread's carry chains are
- * slower than a host core's 64-bit products: about 0.58 ms per call on a B200
+ * slower than a host core's 64-bit products: about 0.55 ms per call on a B200
  * for this library's plain results, against about 0.21 ms for the Horner
  * pass on one host core of the same machine (0.13 ms here for batched
  * results, whose upper bits are infinity).  Use it when the point is wanted
