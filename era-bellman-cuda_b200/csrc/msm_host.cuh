@@ -47,7 +47,8 @@ constexpr unsigned PROFILE_STAGES = 6;
 // Accumulation ranges per thread, handed out to warps dynamically.  Measured
 // on a B200 at 2^22: 2 per thread cut the plain accumulation from 9.85 to
 // 9.32 ms (the last ranges no longer leave SMs idle), 3 gave 9.50 (more heads
-// to merge); the batched chain measured best at 1.
+// to merge); with the warp-scan head merge, at 2^23, 2 / 3 / 4 per thread
+// 18.39 / 18.84 / 18.58 ms.  The batched chain measured best at 1.
 #ifndef ACC_RANGES_PER_THREAD
 #define ACC_RANGES_PER_THREAD 2
 #endif
