@@ -489,6 +489,7 @@ cudaError_t make_batch_plan(batch_plan &b, const base_table_impl *table, const u
     return cudaErrorInvalidValue;
   b = batch_plan{};
   b.instances = instances;
+  b.sms = (unsigned)sms;
   b.inst.resize(instances);
   // instance geometry; reduction groups by window width (buckets of a group contiguous)
   std::map<unsigned, std::vector<unsigned>> by_c;
@@ -681,16 +682,7 @@ cudaError_t enqueue_batch(const batch_plan &b, uint8_t *scratch, cudaStream_t s,
       keys[cur], vals[cur], inst, b.instances, zeros, b.acc_ranges, work, buckets, flags, hb[0], hp[0]);
   CHECK(cudaGetLastError());
   launched++;
-  unsigned heads = b.acc_ranges;
-  int h = 0;
-  while (heads > 1) {
-    const unsigned out = (heads + MERGE_HEADS_PER_WARP - 1) / MERGE_HEADS_PER_WARP;
-    merge_heads_kernel<<<(out * 32 + ACC_THREADS - 1) / ACC_THREADS, ACC_THREADS, 0, s>>>(hb[h], hp[h], heads, buckets, hb[h ^ 1], hp[h ^ 1]);
-    CHECK(cudaGetLastError());
-    launched++;
-    heads = out;
-    h ^= 1;
-  }
+  CHECK(enqueue_merge_heads(hb, hp, b.acc_ranges, buckets, b.sms, s, launched));
   if (forks)
     CHECK(cudaEventRecord(fork_events[0], s));
   for (size_t g = 0; g < b.groups.size(); g++) {

@@ -61,6 +61,7 @@ struct batch_plan {
   unsigned instances = 0;
   unsigned long long total_entries = 0;
   unsigned total_points = 0, total_tiles = 0, total_point_tiles = 0, slots = 0, sort_passes = 0, acc_threads = 0, acc_ranges = 0;
+  unsigned sms = 0; // SMs of the device the plan is for
   std::vector<batch_instance> inst;
   std::vector<batch_group> groups;
   size_t keys[2], vals[2], counts, totals, zeros, buckets, flags, hb[2], hp[2], work, inst_dev, tile_seg_dev, ptile_seg_dev, io;

@@ -548,17 +548,39 @@ static cudaError_t enqueue_accumulation(const plan &p, const fe *scalars, const 
   CHECK(m.mark(stream));
 
   // 5. heads
-  unsigned heads = p.tail_ranges;
+  CHECK(enqueue_merge_heads(hb, hp, p.tail_ranges, buckets, p.sms, stream, m.launched));
+  CHECK(m.mark(stream));
+  return cudaSuccess;
+}
+
+// Levels of at most this many heads per SM (a few warps per SM either way:
+// the launch's time is one chain of dependent additions) take the 4-lane
+// merge, 8 heads per warp with each addition in rounds of independent
+// products.  Every level that way measured slower (2^12: 0.089 -> 0.123 ms,
+// 2^22: 0.081 -> 0.136 ms: more levels); with this threshold the head-merge
+// stage at 2^14 0.136 -> 0.118 ms, at 2^16 0.157 -> 0.146 ms, at 2^22
+// 0.081 -> 0.089 ms.  A choice per level by modelled costs (about 25 us per
+// 32-head level, 14 us per 4-lane level) measured no better overall
+// (0.134 ms at 2^14, 0.084 at 2^22).
+constexpr unsigned MERGE_GROUP4_HEADS_PER_SM = 32;
+
+cudaError_t enqueue_merge_heads(uint32_t *const hb[2], xyzz *const hp[2], unsigned heads, xyzz *buckets, unsigned sms, cudaStream_t stream,
+                                unsigned &launched) {
   int h = 0;
   while (heads > 1) {
-    const unsigned out = (heads + MERGE_HEADS_PER_WARP - 1) / MERGE_HEADS_PER_WARP;
-    merge_heads_kernel<<<(out * 32 + ACC_THREADS - 1) / ACC_THREADS, ACC_THREADS, 0, stream>>>(hb[h], hp[h], heads, buckets, hb[h ^ 1], hp[h ^ 1]);
+    const bool small = heads <= (unsigned long long)sms * MERGE_GROUP4_HEADS_PER_SM;
+    const unsigned per_warp = small ? MERGE_HEADS_PER_WARP_GROUP4 : MERGE_HEADS_PER_WARP;
+    const unsigned out = (heads + per_warp - 1) / per_warp;
+    const unsigned blocks = (unsigned)(((unsigned long long)out * 32 + ACC_THREADS - 1) / ACC_THREADS);
+    if (small)
+      merge_heads_group4_kernel<<<blocks, ACC_THREADS, 0, stream>>>(hb[h], hp[h], heads, buckets, hb[h ^ 1], hp[h ^ 1]);
+    else
+      merge_heads_kernel<<<blocks, ACC_THREADS, 0, stream>>>(hb[h], hp[h], heads, buckets, hb[h ^ 1], hp[h ^ 1]);
     CHECK(cudaGetLastError());
-    m.launched++;
+    launched++;
     heads = out;
     h ^= 1;
   }
-  CHECK(m.mark(stream));
   return cudaSuccess;
 }
 

@@ -65,6 +65,10 @@ constexpr unsigned PROFILE_STAGES = 6;
 // for the gather kernels.  tree / streams: the ping-pong buffers of the plan.
 cudaError_t enqueue_window_sums(const plan &p, const xyzz *buckets, const uint8_t *flags, xyzz *const tree[2], xyzz *const streams[2],
                                 cudaStream_t stream, unsigned &launched);
+// Folds `heads` head partial sums (hb[0], hp[0]; one bucket's heads
+// contiguous) into their buckets, level by level, ping-ponging hb / hp.
+cudaError_t enqueue_merge_heads(uint32_t *const hb[2], xyzz *const hp[2], unsigned heads, xyzz *buckets, unsigned sms, cudaStream_t stream,
+                                unsigned &launched);
 
 unsigned default_window_bits(unsigned long long n);
 // Affine pairing levels by size, and a process-wide override (< 0: by size).

@@ -411,6 +411,59 @@ __global__ void __launch_bounds__(ACC_THREADS) merge_heads_kernel(const uint32_t
     hb_out[w] = INVALID_BUCKET;
 }
 
+// The same merge with 8 heads per warp, one per group of four lanes whose
+// XYZZ additions run in rounds of independent products (msm_group4.cuh):
+// three scan steps over the groups, then the bucket additions.  For the
+// small later levels, where one addition's latency is the launch's.
+__global__ void __launch_bounds__(ACC_THREADS) merge_heads_group4_kernel(const uint32_t *__restrict__ hb_in, const xyzz *__restrict__ hp_in,
+                                                                         unsigned n_in, xyzz *__restrict__ buckets, uint32_t *__restrict__ hb_out,
+                                                                         xyzz *__restrict__ hp_out) {
+  constexpr unsigned GROUPS = MERGE_HEADS_PER_WARP_GROUP4;
+  const unsigned lane = threadIdx.x & 31, g = lane >> 2, role = lane & 3;
+  const unsigned w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if ((unsigned long long)w * GROUPS >= n_in)
+    return; // whole warps only
+  const unsigned long long k = (unsigned long long)w * GROUPS + g;
+  const uint32_t b = k < n_in ? hb_in[k] : INVALID_BUCKET;
+  xyzz acc = b != INVALID_BUCKET ? load_xyzz(hp_in + k) : curve::infinity();
+#pragma unroll
+  for (unsigned d = 1; d < GROUPS; d <<= 1) {
+    const uint32_t bo = __shfl_up_sync(0xffffffffu, b, 4 * d);
+    const xyzz o = shfl_up_xyzz(acc, 4 * d);
+    const bool take = g >= d && bo == b && b != INVALID_BUCKET;
+    if (__any_sync(0xffffffffu, take))
+      acc = select_xyzz(take, add_group4(o, acc), acc);
+  }
+  const uint32_t prev = __shfl_up_sync(0xffffffffu, b, 4), next = __shfl_down_sync(0xffffffffu, b, 4);
+  const unsigned join_lanes = __ballot_sync(0xffffffffu, g > 0 && prev == b); // group g continues group g - 1's segment
+  unsigned joins = 0;
+#pragma unroll
+  for (unsigned f = 0; f < GROUPS; f++)
+    joins |= ((join_lanes >> (4 * f)) & 1u) << f;
+  const unsigned first = 31 - __clz(~joins & ((2u << g) - 1)); // first group of this group's segment
+  const uint32_t b0 = __shfl_sync(0xffffffffu, b, 0);
+  uint32_t before = INVALID_BUCKET;
+  if (lane == 0 && w > 0)
+    before = hb_in[(size_t)w * GROUPS - 1];
+  before = __shfl_sync(0xffffffffu, before, 0);
+  const bool continued = b0 != INVALID_BUCKET && before == b0; // group 0's segment began in an earlier warp
+  const bool ends = b != INVALID_BUCKET && (g == GROUPS - 1 || next != b);
+  const bool out_head = ends && first == 0 && continued;
+  const bool into_bucket = ends && !out_head;
+  const xyzz held = into_bucket ? load_xyzz(buckets + b) : curve::infinity();
+  if (__any_sync(0xffffffffu, into_bucket)) {
+    const xyzz sum = add_group4(held, acc);
+    if (into_bucket && role == 0)
+      store_xyzz(buckets + b, sum);
+  }
+  if (out_head && role == 0) {
+    hb_out[w] = b;
+    store_xyzz(hp_out + w, acc);
+  }
+  if (lane == 0 && !continued)
+    hb_out[w] = INVALID_BUCKET;
+}
+
 // Fold the buckets of one chunk of points into the MSM's buckets (host-resident
 // inputs are processed in chunks whose copies overlap the previous chunk's
 // work).  One thread per bucket slot.

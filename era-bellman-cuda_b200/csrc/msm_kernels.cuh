@@ -192,6 +192,12 @@ __global__ void accumulate_list_kernel(const uint32_t *__restrict__ list_buckets
 constexpr unsigned MERGE_HEADS_PER_WARP = 32;
 __global__ void merge_heads_kernel(const uint32_t *__restrict__ hb_in, const xyzz *__restrict__ hp_in, unsigned n_in, xyzz *__restrict__ buckets,
                                    uint32_t *__restrict__ hb_out, xyzz *__restrict__ hp_out);
+// the same with 8 heads per warp and 4-lane additions (msm_group4.cuh), for
+// levels of at most MERGE_HEADS_GROUP4_MAX heads; launched as one level of a
+// chain of merge launches (enqueue_merge_heads)
+constexpr unsigned MERGE_HEADS_PER_WARP_GROUP4 = 8;
+__global__ void merge_heads_group4_kernel(const uint32_t *__restrict__ hb_in, const xyzz *__restrict__ hp_in, unsigned n_in,
+                                          xyzz *__restrict__ buckets, uint32_t *__restrict__ hb_out, xyzz *__restrict__ hp_out);
 
 // buckets += chunk_buckets for every slot flagged in chunk_flags
 __global__ void merge_chunk_buckets_kernel(xyzz *__restrict__ buckets, uint8_t *__restrict__ flags, const xyzz *__restrict__ chunk_buckets,

@@ -16,30 +16,36 @@ def key_slot(key, B):
     return (key + 1) & (B - 1)
 
 
-def merge_heads_level(hb, hp, heads, buckets):
-    """One merge_heads_kernel launch, lane by lane: warp w takes heads
-    [32 w, 32 w + 32), a segmented Kogge-Stone inclusive scan leaves each
-    segment's sum in its last lane; the segment holding lane 0 is a
-    continuation when the head before the warp has its bucket (-> the warp's
-    output head), every other segment is added into its bucket."""
-    out = (heads + 31) // 32
+MERGE_SMALL_LEVEL = 64  # the model's level size at which the merge takes 8 heads per warp (the kernels': 32 per SM)
+
+
+def merge_heads_level(hb, hp, heads, buckets, per_warp=32):
+    """One merge_heads_kernel launch (per_warp = 32, one head per lane) or
+    merge_heads_group4_kernel launch (per_warp = 8, one head per group of
+    four lanes): warp w takes heads [per_warp w, per_warp (w + 1)), a
+    segmented Kogge-Stone inclusive scan leaves each segment's sum in its
+    last slot; the segment holding slot 0 is a continuation when the head
+    before the warp has its bucket (-> the warp's output head), every other
+    segment is added into its bucket."""
+    P = per_warp
+    out = (heads + P - 1) // P
     hb2, hp2 = [None] * out, [0] * out
     updated = set()
     for w in range(out):
-        b = [hb[32 * w + l] if 32 * w + l < heads else None for l in range(32)]
-        acc = [hp[32 * w + l] if b[l] is not None else 0 for l in range(32)]
+        b = [hb[P * w + l] if P * w + l < heads else None for l in range(P)]
+        acc = [hp[P * w + l] if b[l] is not None else 0 for l in range(P)]
         d = 1
-        while d < 32:
+        while d < P:
             old = list(acc)  # every lane shuffles before any adds
-            for l in range(32):
+            for l in range(P):
                 if l >= d and b[l - d] == b[l] and b[l] is not None:
                     acc[l] = (old[l - d] + old[l]) % R
             d <<= 1
-        joins = [l > 0 and b[l - 1] == b[l] for l in range(32)]
-        before = hb[32 * w - 1] if w > 0 else None
+        joins = [l > 0 and b[l - 1] == b[l] for l in range(P)]
+        before = hb[P * w - 1] if w > 0 else None
         continued = b[0] is not None and before == b[0]
-        for l in range(32):
-            if b[l] is None or (l < 31 and b[l + 1] == b[l]):
+        for l in range(P):
+            if b[l] is None or (l < P - 1 and b[l + 1] == b[l]):
                 continue
             first = max(f for f in range(l + 1) if not joins[f])
             if first == 0 and continued:
@@ -128,7 +134,7 @@ def model_msm(scal, kl, c, T, log_m_max=3):
         for a, b in zip(valid, valid[1:]):
             if hb[a] == hb[b]:
                 assert b == a + 1, "heads of one bucket are not contiguous"
-        hb2, hp2 = merge_heads_level(hb, hp, heads, buckets)
+        hb2, hp2 = merge_heads_level(hb, hp, heads, buckets, 8 if heads <= MERGE_SMALL_LEVEL else 32)
         out = len(hb2)
         hb, hp, heads = hb2, hp2, out
     log_m = min(log_m_max, log_b)
