@@ -225,14 +225,14 @@ __global__ void __launch_bounds__(SORT_THREADS, SORT_SCATTER_MIN_BLOCKS) batch_s
 // instances' tiles interleaved (every instance's local tile j before any
 // instance's tile j + 1), so the tiles in flight spread over the instances
 // and a tile's look-back walks over few aggregates of its own segment; its
-// predecessors took their tickets earlier and are resident.  agg and incl
-// hold 256 counts per global tile, flags one word per global tile (this
-// pass's, zero at launch); totals: the instances' digit totals of this pass.
+// predecessors took their tickets earlier and are resident.  words: 256 per
+// global tile (this pass's, zero at launch); totals: the instances' digit
+// totals of this pass.  Dynamic shared memory lookback_smem_bytes<SORT_THREADS,
+// SORT_ITEMS>().
 __global__ void __launch_bounds__(SORT_THREADS, SORT_SCATTER_MIN_BLOCKS) batch_lookback_kernel(
     const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in, uint32_t *__restrict__ keys_out, uint32_t *__restrict__ vals_out,
     const batch_instance *__restrict__ inst, const unsigned *__restrict__ tile_seg, const unsigned *__restrict__ tile_order, unsigned shift,
-    uint32_t *flags, uint32_t *agg, uint32_t *incl, const uint32_t *__restrict__ totals, const uint32_t *__restrict__ zeros, unsigned *tile_ctr,
-    unsigned *error) {
+    uint32_t *words, const uint32_t *__restrict__ totals, const uint32_t *__restrict__ zeros, unsigned *tile_ctr, unsigned *error) {
   __shared__ unsigned s_ticket;
   if (threadIdx.x == 0)
     s_ticket = atomicAdd(tile_ctr, 1u);
@@ -244,9 +244,8 @@ __global__ void __launch_bounds__(SORT_THREADS, SORT_SCATTER_MIN_BLOCKS) batch_l
   const unsigned skip = zeros[k], live = d.entries - skip;
   if (base >= live) // no later tile of this segment holds entries either, so none waits for this one
     return;
-  const size_t rows = (size_t)d.tile_base * SORT_RADIX;
-  lookback_tile(keys_in, vals_in, keys_out, vals_out, d.entry_offset + skip, local, min(SORT_TILE, live - base), shift, flags + d.tile_base,
-                agg + rows, incl + rows, totals + (size_t)k * SORT_RADIX, error);
+  lookback_tile<SORT_THREADS, SORT_ITEMS>(keys_in, vals_in, keys_out, vals_out, d.entry_offset + skip, local, min(SORT_TILE, live - base), shift,
+                                          words + (size_t)d.tile_base * SORT_RADIX, totals + (size_t)k * SORT_RADIX, error);
 }
 
 // The batch's segments for accumulate_ranges: one per instance.
@@ -562,19 +561,20 @@ cudaError_t make_batch_plan(batch_plan &b, const base_table_impl *table, const u
     b.keys[i] = take(b.total_entries * 4);
     b.vals[i] = take(b.total_entries * 4);
   }
-  // the first pass's tile counts, reused by the later passes as the tiles'
-  // look-back aggregates; the look-back inclusive counts
+  // the first pass's tile counts, then (cleared after that pass) the first
+  // later pass's look-back words, 256 per tile; the second later pass's
+  // look-back words (cleared before that pass)
+  static_assert((MAX_TABLE_BITS - 1 + SORT_RADIX_BITS - 1) / SORT_RADIX_BITS <= 3, "two look-back word arrays: at most three radix passes");
   b.counts = take((size_t)b.total_tiles * SORT_RADIX * 4);
-  b.incl = b.sort_passes > 1 ? take((size_t)b.total_tiles * SORT_RADIX * 4) : 0;
+  b.words2 = b.sort_passes > 2 ? take((size_t)b.total_tiles * SORT_RADIX * 4) : 0;
   b.totals = take((size_t)instances * SORT_RADIX * 4);
   // cleared every execution: zero digits per instance, the later passes'
-  // digit totals per instance, their look-back flags per tile, a tile ticket
-  // counter per later pass and the look-back error word
+  // digit totals per instance, a tile ticket counter per later pass and the
+  // look-back error word
   const unsigned later = b.sort_passes - 1;
-  b.zeros = take(((size_t)instances + (size_t)later * instances * SORT_RADIX + (size_t)later * b.total_tiles + later + 1) * 4);
+  b.zeros = take(((size_t)instances + (size_t)later * instances * SORT_RADIX + later + 1) * 4);
   b.later_totals = b.zeros + (size_t)instances * 4;
-  b.lookback_flags = b.later_totals + (size_t)later * instances * SORT_RADIX * 4;
-  b.sort_ctrs = b.lookback_flags + (size_t)later * b.total_tiles * 4;
+  b.sort_ctrs = b.later_totals + (size_t)later * instances * SORT_RADIX * 4;
   b.sort_error = b.sort_ctrs + (size_t)later * 4;
   b.sort_clear_bytes = b.sort_error + 4 - b.zeros;
   b.buckets = take((size_t)b.slots * sizeof(xyzz));
@@ -663,15 +663,16 @@ cudaError_t enqueue_batch(const batch_plan &b, uint8_t *scratch, cudaStream_t s,
   CHECK(cudaGetLastError());
   launched += 2;
   int cur = 1;
-  // later passes: one look-back kernel each
+  // later passes: one look-back kernel each, on words cleared before it
   const unsigned *tile_order = reinterpret_cast<const unsigned *>(at(b.tile_order_dev));
-  uint32_t *lookback_flags = reinterpret_cast<uint32_t *>(at(b.lookback_flags)), *incl = reinterpret_cast<uint32_t *>(at(b.incl));
   unsigned *sort_ctrs = reinterpret_cast<unsigned *>(at(b.sort_ctrs)), *sort_error = reinterpret_cast<unsigned *>(at(b.sort_error));
+  const size_t word_bytes = (size_t)b.total_tiles * SORT_RADIX * 4;
   for (unsigned pass = 1; pass < b.sort_passes; pass++) {
-    batch_lookback_kernel<<<b.total_tiles, SORT_THREADS, 0, s>>>(
-        keys[cur], vals[cur], keys[cur ^ 1], vals[cur ^ 1], inst, tile_seg, tile_order, pass * SORT_RADIX_BITS,
-        lookback_flags + (size_t)(pass - 1) * b.total_tiles, counts, incl, later_totals + (size_t)(pass - 1) * b.instances * SORT_RADIX, zeros,
-        sort_ctrs + pass - 1, sort_error);
+    uint32_t *words = pass == 1 ? counts : reinterpret_cast<uint32_t *>(at(b.words2));
+    CHECK(cudaMemsetAsync(words, 0, word_bytes, s));
+    batch_lookback_kernel<<<b.total_tiles, SORT_THREADS, lookback_smem_bytes<SORT_THREADS, SORT_ITEMS>(), s>>>(
+        keys[cur], vals[cur], keys[cur ^ 1], vals[cur ^ 1], inst, tile_seg, tile_order, pass * SORT_RADIX_BITS, words,
+        later_totals + (size_t)(pass - 1) * b.instances * SORT_RADIX, zeros, sort_ctrs + pass - 1, sort_error);
     CHECK(cudaGetLastError());
     launched++;
     cur ^= 1;

@@ -66,7 +66,7 @@ struct batch_plan {
   std::vector<batch_group> groups;
   size_t keys[2], vals[2], counts, totals, zeros, buckets, flags, hb[2], hp[2], work, inst_dev, tile_seg_dev, ptile_seg_dev, io;
   // the look-back passes (all offsets; the zeros .. sort_error range is cleared every execution)
-  size_t incl = 0, later_totals = 0, lookback_flags = 0, sort_ctrs = 0, sort_error = 0, sort_clear_bytes = 0, tile_order_dev = 0;
+  size_t words2 = 0, later_totals = 0, sort_ctrs = 0, sort_error = 0, sort_clear_bytes = 0, tile_order_dev = 0;
   size_t digit_smem = 0; // dynamic shared memory of the digit kernel (its widest instance)
   size_t bytes = 0;       // scratch bytes
   size_t descriptors = 0; // offset of the constant descriptors (inst_dev .. end of members)

@@ -267,17 +267,12 @@ __device__ __forceinline__ void scan_256(const uint32_t *in, uint32_t *out, uint
 // RUN_BASES fills glob[d] (d < SORT_RADIX), the position of this tile's run
 // of digit d relative to seg_out, from the tile's digit counts tile_cnt[]; it
 // is called by every thread of the block (it may synchronise the block) and
-// may use digit_base[] and warp_sums[] as scratch.  AFTER() runs on every
-// thread once glob[] is complete, before the tile is staged and written.
-struct no_op {
-  __device__ __forceinline__ void operator()() const {}
-};
-template <bool STABLE, bool DROP_ZEROS, class RUN_BASES, class AFTER = no_op>
+// may use digit_base[] and warp_sums[] as scratch.
+template <bool STABLE, bool DROP_ZEROS, class RUN_BASES>
 __device__ __forceinline__ void scatter_tile(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in, uint32_t *__restrict__ keys_out,
                                              uint32_t *__restrict__ vals_out, size_t seg_in, size_t seg_out, unsigned base, unsigned count,
-                                             unsigned shift, RUN_BASES run_bases, AFTER after = AFTER()) {
-  __shared__ uint32_t s_key[SORT_TILE];
-  __shared__ uint32_t s_val[SORT_TILE];
+                                             unsigned shift, RUN_BASES run_bases) {
+  __shared__ uint2 s_kv[SORT_TILE]; // the staged tile, key and value in one 8-byte word
   __shared__ uint32_t whist[STABLE ? SORT_WARPS : 1][SORT_RADIX];
   __shared__ uint32_t tile_cnt[SORT_RADIX], tile_off[SORT_RADIX], glob[SORT_RADIX], digit_base[SORT_RADIX], warp_sums[SORT_WARPS];
   __shared__ uint32_t staged;
@@ -340,15 +335,16 @@ __device__ __forceinline__ void scatter_tile(const uint32_t *__restrict__ keys_i
     staged = tile_off[SORT_RADIX - 1] + tile_cnt[SORT_RADIX - 1]; // items kept (dropped zero keys excluded)
   run_bases(static_cast<const uint32_t *>(tile_cnt), glob, digit_base, warp_sums);
   __syncthreads();
-  after();
+  // glob[d] becomes the offset from a staged position to its output
+  // position (mod 2^32; the output position itself is below 2^32)
+  for (unsigned d = threadIdx.x; d < SORT_RADIX; d += blockDim.x)
+    glob[d] -= tile_off[d];
 #pragma unroll
   for (unsigned r = 0; r < SORT_ITEMS; r++) {
     const unsigned i = sub + r * 32 + lane;
     if (i < count && (!DROP_ZEROS || key[r] != ZERO_KEY)) {
       const unsigned d = sort_digit(key[r], shift);
-      const unsigned pos = tile_off[d] + (STABLE ? whist[warp][d] : 0) + rank[r];
-      s_key[pos] = key[r];
-      s_val[pos] = val[r];
+      s_kv[tile_off[d] + (STABLE ? whist[warp][d] : 0) + rank[r]] = make_uint2(key[r], val[r]);
     }
   }
   __syncthreads();
@@ -356,11 +352,10 @@ __device__ __forceinline__ void scatter_tile(const uint32_t *__restrict__ keys_i
   for (unsigned j = 0; j < SORT_ITEMS; j++) {
     const unsigned pos = j * SORT_THREADS + threadIdx.x;
     if (pos < staged) {
-      const uint32_t k = s_key[pos];
-      const unsigned d = sort_digit(k, shift);
-      const size_t out = seg_out + glob[d] + (pos - tile_off[d]);
-      keys_out[out] = k;
-      vals_out[out] = s_val[pos];
+      const uint2 kv = s_kv[pos];
+      const size_t out = seg_out + (uint32_t)(glob[sort_digit(kv.x, shift)] + pos);
+      keys_out[out] = kv.x;
+      vals_out[out] = kv.y;
     }
   }
 }
@@ -386,125 +381,205 @@ __device__ __forceinline__ void sort_scatter_tile(const uint32_t *__restrict__ k
 }
 
 // ---------------------------------------------------------------------------
-// stable radix passes in one kernel, with decoupled look-back (the plain
-// pipeline's passes after the first)
+// stable radix passes in one kernel, with decoupled look-back (the passes
+// after the first, plain and batched pipelines)
 // ---------------------------------------------------------------------------
-// Per (window, tile): a flag word -- LOOKBACK_NONE, LOOKBACK_AGGREGATE (the
-// tile's own digit counts are in agg[tile][0..255]) or LOOKBACK_INCLUSIVE (the
-// counts over this and every earlier tile of the window are in
-// incl[tile][0..255]).  The counts are written first and made visible
-// (__threadfence) before the flag is set; readers load the flag with acquire
-// semantics before the counts.
-constexpr uint32_t LOOKBACK_NONE = 0, LOOKBACK_AGGREGATE = 1, LOOKBACK_INCLUSIVE = 2;
-// Polls of a batch of predecessors, one of which has published nothing yet,
-// before a wait gives up (well under a second with the back-off below).  A
-// predecessor took its tile earlier from the same counter, so it is resident
-// and publishes its counts right after ranking: in correct operation the wait
-// ends within microseconds; the limit only keeps a failure from hanging the
-// GPU.
+// Per (segment, tile, digit) one 32-bit word: a status in the top two bits --
+// none yet (0), LOOKBACK_AGGREGATE (the low 30 bits are the tile's own count
+// of the digit) or LOOKBACK_INCLUSIVE (the count over this and every earlier
+// tile of the segment) -- and the count below it.  A reader sees status and
+// count together in one load, so publishing needs no fence, and each digit
+// is looked back on its own.  The words start at zero (cleared before each
+// pass); counts stay below 2^30 because a segment holds at most 2^29 + 2^5
+// entries (chunks of at most 2^29 points; batch instances are smaller).
+constexpr uint32_t LOOKBACK_AGGREGATE = 1u << 30, LOOKBACK_INCLUSIVE = 2u << 30, LOOKBACK_COUNT = LOOKBACK_AGGREGATE - 1;
+// Polls of a predecessor's word that is still empty before a wait gives up
+// (well under a second with the back-off below).  A predecessor took its tile
+// earlier from the same ticket counter, so it is resident and publishes right
+// after ranking: in correct operation the wait ends within microseconds; the
+// limit only keeps a failure from hanging the GPU.
 constexpr unsigned LOOKBACK_MAX_POLLS = 1u << 20;
-constexpr int LOOKBACK_GAVE_UP = -2;
-static_assert(SORT_THREADS == SORT_RADIX, "look-back: one digit per thread");
+// Predecessor words one look-back step loads together (independent loads, so
+// a walk over a few aggregates costs one or two round trips to L2).
+constexpr unsigned LOOKBACK_BATCH = 8;
+static_assert(SORT_RADIX == 256, "look-back: one digit per thread of the first 256");
 
-__device__ __forceinline__ uint32_t load_acquire(const uint32_t *p) {
-  uint32_t v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
 __device__ __forceinline__ uint32_t load_relaxed(const uint32_t *p) {
   uint32_t v;
   asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
 }
-__device__ __forceinline__ void store_release(uint32_t *p, uint32_t v) { asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory"); }
+__device__ __forceinline__ void store_relaxed(uint32_t *p, uint32_t v) { asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory"); }
 
-// Publishes this tile's digit counts src[0..255] (shared memory) under
-// `flag`: the first warp writes them (eight per lane), makes its writes
-// visible device-wide, then sets the flag.  Called by the first warp only.
-__device__ __forceinline__ void lookback_publish(uint32_t *flags, uint32_t *counts, unsigned tile, const uint32_t *src, uint32_t flag) {
-  const unsigned lane = threadIdx.x & 31;
-  uint32_t *row = counts + (size_t)tile * SORT_RADIX;
+// Digit d's count over the tiles before `tile` of its segment (words: the
+// segment's [tiles][256] words, column d).  The tile's own count `own` is
+// published first (tile 0 publishes it as inclusive at once); then earlier
+// words are read LOOKBACK_BATCH at a time, newest first, adding counts until
+// an inclusive one; an empty word means that tile has not ranked yet and is
+// polled again (bounded).  Finally the inclusive count is published.  A wait
+// that gives up sets *error and returns what it has added so far: a smaller
+// prefix only moves this tile's (and its successors') positions down, so
+// every write stays inside the segment, the kernel ends and *error reports
+// the wrong order.
+__device__ __forceinline__ uint32_t lookback_digit(uint32_t *words, unsigned tile, unsigned d, uint32_t own, unsigned *error) {
+  uint32_t *mine = words + (size_t)tile * SORT_RADIX + d;
+  if (tile == 0) {
+    store_relaxed(mine, LOOKBACK_INCLUSIVE | own);
+    return 0;
+  }
+  store_relaxed(mine, LOOKBACK_AGGREGATE | own);
+  uint32_t prefix = 0;
+  int j = (int)tile - 1; // newest tile not yet added
+  unsigned polls = 0;
+  bool done = false;
+  while (!done) {
+    uint32_t v[LOOKBACK_BATCH];
 #pragma unroll
-  for (unsigned k = 0; k < SORT_RADIX / 32; k++)
-    row[k * 32 + lane] = src[k * 32 + lane];
-  __threadfence();
-  __syncwarp();
-  if (lane == 0)
-    store_release(flags + tile, flag);
+    for (unsigned k = 0; k < LOOKBACK_BATCH; k++) // before tile 0: an inclusive count of zero
+      v[k] = j - (int)k >= 0 ? load_relaxed(words + (size_t)(j - (int)k) * SORT_RADIX + d) : LOOKBACK_INCLUSIVE;
+    bool empty = false;
+#pragma unroll
+    for (unsigned k = 0; k < LOOKBACK_BATCH; k++) {
+      if (!done && !empty) {
+        if (v[k] < LOOKBACK_AGGREGATE) {
+          empty = true;
+        } else {
+          prefix += v[k] & LOOKBACK_COUNT;
+          done = v[k] >= LOOKBACK_INCLUSIVE;
+          j--;
+        }
+      }
+    }
+    if (empty) {
+      if (++polls == LOOKBACK_MAX_POLLS) {
+        atomicOr(error, 1u);
+        break;
+      }
+      __nanosleep(100);
+    }
+  }
+  store_relaxed(mine, LOOKBACK_INCLUSIVE | (prefix + own));
+  return prefix;
 }
 
-// One stable radix pass over one tile of a window segment, with run
-// positions found by decoupled look-back over the window's earlier tiles:
-// after ranking, the tile publishes its aggregate; the first warp then reads
-// the flags of the 32 nearest earlier tiles at a time until it finds one with
-// an inclusive count (waiting, bounded, while a tile between has published
-// nothing), and every thread adds that inclusive count and the aggregates
-// after it for its digit; the tile then publishes its own inclusive count.
-// totals: the window's digit totals.  A wait that gives up sets *error and
-// uses what it has (positions then only shrink, so every write stays inside
-// the segment): the kernel always ends; the sort is wrong and *error says so.
+// Exclusive scans over the 256 digits of two sets of values at once (thread
+// d < 256 passes a[d] and b[d]; other threads pass zeros): one block barrier.
+// Every thread of the block must call; each block calls it once.
+__device__ __forceinline__ uint2 scan2_256(uint32_t a, uint32_t b) {
+  __shared__ uint2 warp_sums[SORT_RADIX / 32];
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t ia = a, ib = b;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const uint32_t ua = __shfl_up_sync(0xffffffffu, ia, off), ub = __shfl_up_sync(0xffffffffu, ib, off);
+    if (lane >= (unsigned)off) {
+      ia += ua;
+      ib += ub;
+    }
+  }
+  if (threadIdx.x < SORT_RADIX && lane == 31)
+    warp_sums[warp] = make_uint2(ia, ib);
+  __syncthreads();
+  uint32_t ba = 0, bb = 0;
+  if (threadIdx.x < SORT_RADIX)
+    for (unsigned k = 0; k < warp; k++) {
+      ba += warp_sums[k].x;
+      bb += warp_sums[k].y;
+    }
+  return make_uint2(ba + ia - a, bb + ib - b);
+}
+
+// One stable radix pass over one tile of `count` entries (at most THREADS *
+// ITEMS) at seg + base, base = tile * THREADS * ITEMS, written to the same
+// segment of the output arrays.  Ranks among equal digits warp by warp, 32
+// consecutive items per round (warp_peers), then per digit: the prefix over
+// warps, the tile's count published and the count over earlier tiles found
+// by look-back (lookback_digit; the first 256 threads, one digit each), the
+// digit's run position = its total over smaller digits (totals: the
+// segment's digit totals) + that prefix.  The tile is then reordered in
+// shared memory so that each digit's run is written with consecutive
+// addresses.  Needs lookback_smem_bytes<THREADS, ITEMS>() of dynamic shared
+// memory.
+template <unsigned THREADS, unsigned ITEMS>
 __device__ __forceinline__ void lookback_tile(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
                                               uint32_t *__restrict__ keys_out, uint32_t *__restrict__ vals_out, size_t seg, unsigned tile,
-                                              unsigned count, unsigned shift, uint32_t *flags, uint32_t *agg, uint32_t *incl,
-                                              const uint32_t *__restrict__ totals, unsigned *error) {
-  __shared__ uint32_t s_incl[SORT_RADIX]; // this tile's inclusive counts, published after the bases are known
-  scatter_tile<true, false>(
-      keys_in, vals_in, keys_out, vals_out, seg, seg, tile * SORT_TILE, count, shift,
-      [&](const uint32_t *tile_cnt, uint32_t *glob, uint32_t *digit_base, uint32_t *warp_sums) {
-        __shared__ int s_start;
-        const unsigned d = threadIdx.x, lane = threadIdx.x & 31;
-        const uint32_t own = tile_cnt[d];
-        if (threadIdx.x < 32) {
-          lookback_publish(flags, agg, tile, tile_cnt, LOOKBACK_AGGREGATE);
-          int hi = (int)tile; // tiles [0, hi) are still to be examined
-          int start = -1;     // nearest earlier tile with an inclusive count
-          unsigned polls = 0;
-          while (hi > 0) {
-            const int j = hi - 1 - (int)lane;
-            const uint32_t f = j >= 0 ? load_acquire(flags + j) : LOOKBACK_AGGREGATE;
-            const unsigned inclusive = __ballot_sync(0xffffffffu, f == LOOKBACK_INCLUSIVE);
-            const unsigned missing = __ballot_sync(0xffffffffu, f == LOOKBACK_NONE);
-            const unsigned nearest = inclusive ? __ffs(inclusive) - 1 : 32;
-            const unsigned before = nearest == 32 ? 0xffffffffu : (1u << nearest) - 1;
-            if (missing & before) {
-              if (++polls == LOOKBACK_MAX_POLLS) {
-                if (lane == 0)
-                  atomicOr(error, 1u);
-                start = LOOKBACK_GAVE_UP;
-                break;
-              }
-              __nanosleep(100);
-              continue;
-            }
-            if (nearest < 32) {
-              start = hi - 1 - (int)nearest;
-              break;
-            }
-            hi -= 32;
-          }
-          if (lane == 0)
-            s_start = start;
-        }
-        glob[d] = totals[d];
-        __syncthreads();
-        scan_256(glob, digit_base, warp_sums); // digit bases of this segment
-        const int start = s_start;
-        uint32_t prefix = start >= 0 ? load_relaxed(incl + (size_t)start * SORT_RADIX + d) : 0;
-        if (start != LOOKBACK_GAVE_UP) {
-          for (int j = start + 1; j < (int)tile; j++)
-            prefix += load_relaxed(agg + (size_t)j * SORT_RADIX + d);
-        } else { // add what the earlier tiles have published
-          for (int j = 0; j < (int)tile; j++)
-            if (load_relaxed(flags + j) != LOOKBACK_NONE)
-              prefix += load_relaxed(agg + (size_t)j * SORT_RADIX + d);
-        }
-        glob[d] = digit_base[d] + prefix;
-        s_incl[d] = prefix + own;
-      },
-      [&] { // the first warp publishes the inclusive counts; the others go on
-        if (threadIdx.x < 32)
-          lookback_publish(flags, incl, tile, s_incl, LOOKBACK_INCLUSIVE);
-      });
+                                              unsigned count, unsigned shift, uint32_t *words, const uint32_t *__restrict__ totals,
+                                              unsigned *error) {
+  constexpr unsigned TILE = THREADS * ITEMS, WARPS = THREADS / 32;
+  static_assert(THREADS >= SORT_RADIX && THREADS % 32 == 0, "look-back tile: at least one thread per digit");
+  extern __shared__ uint2 lookback_shared[];
+  uint2 *s_kv = lookback_shared;
+  uint32_t(*whist)[SORT_RADIX] = reinterpret_cast<uint32_t(*)[SORT_RADIX]>(lookback_shared + TILE);
+  __shared__ uint32_t tile_off[SORT_RADIX], delta[SORT_RADIX];
+  __shared__ uint32_t staged;
+  const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned sub = warp * (32 * ITEMS); // this warp's items: base + sub + r*32 + lane
+  const size_t base = (size_t)tile * TILE;
+  for (unsigned d = lane; d < SORT_RADIX; d += 32)
+    whist[warp][d] = 0;
+  __syncthreads();
+  uint32_t key[ITEMS], val[ITEMS], rank[ITEMS];
+  const unsigned lt_mask = (1u << lane) - 1;
+  // every item's loads first, so that all of them are in flight together
+#pragma unroll
+  for (unsigned r = 0; r < ITEMS; r++) {
+    const unsigned i = sub + r * 32 + lane;
+    key[r] = i < count ? keys_in[seg + base + i] : 0;
+    val[r] = i < count ? vals_in[seg + base + i] : 0;
+  }
+#pragma unroll
+  for (unsigned r = 0; r < ITEMS; r++) {
+    const unsigned i = sub + r * 32 + lane;
+    const bool valid = i < count;
+    const unsigned d = valid ? sort_digit(key[r], shift) : SORT_RADIX;
+    const unsigned peers = warp_peers(d);
+    const uint32_t before = valid ? whist[warp][d] : 0;
+    __syncwarp();
+    if (valid && lane == (unsigned)(__ffs(peers) - 1))
+      whist[warp][d] = before + __popc(peers);
+    __syncwarp();
+    rank[r] = before + __popc(peers & lt_mask);
+  }
+  __syncthreads();
+  uint32_t own = 0, prefix = 0, total = 0;
+  if (threadIdx.x < SORT_RADIX) {
+    const unsigned d = threadIdx.x;
+#pragma unroll
+    for (unsigned k = 0; k < WARPS; k++) { // per digit: exclusive prefix over warps (warp order = item order)
+      const uint32_t t = whist[k][d];
+      whist[k][d] = own;
+      own += t;
+    }
+    prefix = lookback_digit(words, tile, d, own, error);
+    total = totals[d];
+  }
+  const uint2 ex = scan2_256(own, total); // the tile's runs; the segment's digit bases
+  if (threadIdx.x < SORT_RADIX) {
+    tile_off[threadIdx.x] = ex.x;
+    delta[threadIdx.x] = ex.y + prefix - ex.x; // output position - staged position
+    if (threadIdx.x == SORT_RADIX - 1)
+      staged = ex.x + own;
+  }
+  __syncthreads();
+#pragma unroll
+  for (unsigned r = 0; r < ITEMS; r++) {
+    const unsigned i = sub + r * 32 + lane;
+    if (i < count) {
+      const unsigned d = sort_digit(key[r], shift);
+      s_kv[tile_off[d] + whist[warp][d] + rank[r]] = make_uint2(key[r], val[r]);
+    }
+  }
+  __syncthreads();
+#pragma unroll 4
+  for (unsigned j = 0; j < ITEMS; j++) {
+    const unsigned pos = j * THREADS + threadIdx.x;
+    if (pos < staged) {
+      const uint2 kv = s_kv[pos];
+      const size_t out = seg + (uint32_t)(delta[sort_digit(kv.x, shift)] + pos);
+      keys_out[out] = kv.x;
+      vals_out[out] = kv.y;
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------

@@ -159,6 +159,7 @@ plan make_plan(unsigned n, unsigned window_bits, int sms) {
   p.key_bits = p.c - 1; // keys are |d| - 1 for |d| in [1, 2^(c-1)]
   p.sort_passes = (p.key_bits + SORT_RADIX_BITS - 1) / SORT_RADIX_BITS;
   p.tiles = (n + SORT_TILE - 1) / SORT_TILE;
+  p.lookback_tiles = (n + LOOKBACK_TILE - 1) / LOOKBACK_TILE;
   // One accumulation range per resident thread (4 blocks of ACC_THREADS per
   // SM), fewer for small inputs so that every range has work.
   const unsigned long long entries = (unsigned long long)p.windows * n;
@@ -272,7 +273,7 @@ static chunking equal_chunks(unsigned n, unsigned max_chunk, bool copy_inputs) {
 // chunk slots); a chunked MSM holds a second bucket set for the chunks after
 // the first.
 struct layout {
-  size_t keys[2], vals[2], counts, totals, zeros, sort_ctrs, sort_error, lookback_flags, sort_small_bytes, lookback_agg, lookback_incl, buckets, flags,
+  size_t keys[2], vals[2], counts, totals, zeros, sort_ctrs, sort_error, lookback_words, sort_clear_bytes, buckets, flags,
       chunk_buckets, chunk_flags, hb[2], hp[2], work, tree[2], streams[2], results, scalars, bases, total;
   // affine pairing levels: two output lists (level L writes list (L - 1) & 1),
   // the per-pair prefix products, the per-lane and per-warp arrays, and each
@@ -297,21 +298,19 @@ static layout make_layout(const plan &p, bool copy_scalars, bool copy_bases, boo
     l.keys[i] = take(entries * 4);
     l.vals[i] = take(entries * 4);
   }
-  // the first pass's digit counts per (window, digit, tile); then one region cleared per
-  // chunk: digit totals per (pass, window, digit), zero digits per window, a
-  // tile counter per pass, the look-back error word and the look-back flags
-  // of the passes after the first; then the look-back counts (shared by those
-  // passes)
-  const size_t lookback_words = (size_t)p.windows * p.tiles;
+  // the first pass's digit counts per (window, digit, tile); then one region
+  // cleared per chunk: digit totals per (pass, window, digit), zero digits
+  // per window, a tile counter per pass, the look-back error word, and the
+  // look-back words of the passes after the first, per (window, look-back
+  // tile, digit)
+  const size_t lookback_words = (size_t)p.windows * p.lookback_tiles * SORT_RADIX;
   l.counts = take((size_t)p.windows * SORT_RADIX * p.tiles * 4);
-  l.sort_small_bytes = ((size_t)p.sort_passes * p.windows * SORT_RADIX + p.windows + p.sort_passes + 1 + (p.sort_passes - 1) * lookback_words) * 4;
-  l.totals = take(l.sort_small_bytes);
+  l.sort_clear_bytes = ((size_t)p.sort_passes * p.windows * SORT_RADIX + p.windows + p.sort_passes + 1 + (p.sort_passes - 1) * lookback_words) * 4;
+  l.totals = take(l.sort_clear_bytes);
   l.zeros = l.totals + (size_t)p.sort_passes * p.windows * SORT_RADIX * 4;
   l.sort_ctrs = l.zeros + (size_t)p.windows * 4;
   l.sort_error = l.sort_ctrs + (size_t)p.sort_passes * 4;
-  l.lookback_flags = l.sort_error + 4;
-  l.lookback_agg = p.sort_passes > 1 ? take(lookback_words * SORT_RADIX * 4) : 0;
-  l.lookback_incl = p.sort_passes > 1 ? take(lookback_words * SORT_RADIX * 4) : 0;
+  l.lookback_words = l.sort_error + 4;
   const size_t slots = (size_t)p.windows << p.log_b;
   l.buckets = take(slots * sizeof(xyzz));
   l.flags = take(slots);
@@ -430,7 +429,7 @@ static cudaError_t enqueue_accumulation(const plan &p, const fe *scalars, const 
 
   unsigned *sort_ctrs = reinterpret_cast<unsigned *>(scratch + l.sort_ctrs);
   unsigned *sort_error = reinterpret_cast<unsigned *>(scratch + l.sort_error);
-  CHECK(cudaMemsetAsync(totals, 0, l.sort_small_bytes, stream));
+  CHECK(cudaMemsetAsync(totals, 0, l.sort_clear_bytes, stream));
   int cur = 0;
   if (p.windows <= MAX_FUSED_HISTOGRAM_WINDOWS && p.tiles >= FUSED_DIGITS_MIN_TILES) {
     // 1. digits, with every pass's digit counts per tile
@@ -450,12 +449,11 @@ static cudaError_t enqueue_accumulation(const plan &p, const fe *scalars, const 
     CHECK(cudaGetLastError());
     m.launched += 2;
     cur = 1;
-    uint32_t *lookback_flags = reinterpret_cast<uint32_t *>(scratch + l.lookback_flags);
-    uint32_t *agg = reinterpret_cast<uint32_t *>(scratch + l.lookback_agg), *incl = reinterpret_cast<uint32_t *>(scratch + l.lookback_incl);
+    uint32_t *words = reinterpret_cast<uint32_t *>(scratch + l.lookback_words);
     for (unsigned pass = 1; pass < p.sort_passes; pass++) {
-      lookback_stable_kernel<<<p.windows * p.tiles, SORT_THREADS, 0, stream>>>(
-          keys[cur], vals[cur], keys[cur ^ 1], vals[cur ^ 1], n, p.windows, p.tiles, pass * SORT_RADIX_BITS,
-          lookback_flags + (size_t)(pass - 1) * p.windows * p.tiles, agg, incl, totals + (size_t)pass * prefix_rows, zeros, sort_ctrs + pass,
+      lookback_stable_kernel<<<p.windows * p.lookback_tiles, LOOKBACK_THREADS, lookback_smem_bytes<LOOKBACK_THREADS, LOOKBACK_ITEMS>(), stream>>>(
+          keys[cur], vals[cur], keys[cur ^ 1], vals[cur ^ 1], n, p.windows, p.lookback_tiles, pass * SORT_RADIX_BITS,
+          words + (size_t)(pass - 1) * p.windows * p.lookback_tiles * SORT_RADIX, totals + (size_t)pass * prefix_rows, zeros, sort_ctrs + pass,
           sort_error);
       CHECK(cudaGetLastError());
       m.launched++;
@@ -935,6 +933,7 @@ template <class F> static cudaError_t set_carveout(F *func, int percent) {
 cudaError_t set_up() {
   CHECK(cudaFuncSetAttribute(digits_histogram_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_digit_histogram_smem()));
   CHECK(set_carveout(accumulate_kernel, ACC_CARVEOUT)); // 4 blocks x 19 KB of base-point slots and window bounds
+  CHECK(set_carveout(lookback_stable_kernel, cudaSharedmemCarveoutMaxShared)); // 4 blocks x 42 KB
   CHECK(set_carveout(merge_heads_kernel, cudaSharedmemCarveoutMaxL1));
   CHECK(set_carveout(reduce_groups_kernel, cudaSharedmemCarveoutMaxL1));
   CHECK(set_carveout(reduce_level_kernel, cudaSharedmemCarveoutMaxL1));

@@ -92,25 +92,24 @@ __global__ void __launch_bounds__(SORT_THREADS) digits_histogram_kernel(const fe
 // *tile_ctr (0 at launch), so every tile a block waits for belongs to a block
 // that is already running; consecutive tickets go to different windows
 // (ticket = tile * windows + w), so the tiles in flight spread over all
-// windows and each window's look-back stays short.  Per window: flags[tiles],
-// agg and incl [tiles][256], totals[256].
-__global__ void __launch_bounds__(SORT_THREADS, SORT_SCATTER_MIN_BLOCKS)
+// windows and each window's look-back stays short.  Per window: words
+// [tiles][256] (look-back tiles of LOOKBACK_TILE entries), totals[256].
+__global__ void __launch_bounds__(LOOKBACK_THREADS, SORT_SCATTER_MIN_BLOCKS)
     lookback_stable_kernel(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in, uint32_t *__restrict__ keys_out,
-                           uint32_t *__restrict__ vals_out, unsigned n, unsigned windows, unsigned tiles, unsigned shift, uint32_t *flags,
-                           uint32_t *agg, uint32_t *incl, const uint32_t *__restrict__ totals, const uint32_t *__restrict__ zeros,
-                           unsigned *tile_ctr, unsigned *error) {
+                           uint32_t *__restrict__ vals_out, unsigned n, unsigned windows, unsigned tiles, unsigned shift, uint32_t *words,
+                           const uint32_t *__restrict__ totals, const uint32_t *__restrict__ zeros, unsigned *tile_ctr, unsigned *error) {
   __shared__ unsigned s_ticket;
   if (threadIdx.x == 0)
     s_ticket = atomicAdd(tile_ctr, 1u);
   __syncthreads();
   const unsigned w = s_ticket % windows, tile = s_ticket / windows;
   const unsigned skip = zeros[w], live = n - skip;
-  const unsigned base = tile * SORT_TILE;
+  const unsigned base = tile * LOOKBACK_TILE;
   if (base >= live) // no later tile of this window holds entries either, so none waits for this one
     return;
-  const size_t rows = (size_t)w * tiles * SORT_RADIX;
-  lookback_tile(keys_in, vals_in, keys_out, vals_out, w * window_stride(n) + skip, tile, min(SORT_TILE, live - base), shift,
-                flags + (size_t)w * tiles, agg + rows, incl + rows, totals + (size_t)w * SORT_RADIX, error);
+  lookback_tile<LOOKBACK_THREADS, LOOKBACK_ITEMS>(keys_in, vals_in, keys_out, vals_out, w * window_stride(n) + skip, tile,
+                                                  min(LOOKBACK_TILE, live - base), shift, words + (size_t)w * tiles * SORT_RADIX,
+                                                  totals + (size_t)w * SORT_RADIX, error);
 }
 
 // ---------------------------------------------------------------------------

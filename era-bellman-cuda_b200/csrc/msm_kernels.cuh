@@ -63,6 +63,20 @@ constexpr unsigned SORT_TILE = SORT_THREADS * SORT_ITEMS;
 #ifndef SORT_SCATTER_MIN_BLOCKS
 #define SORT_SCATTER_MIN_BLOCKS 4
 #endif
+// The look-back passes (the radix passes after the first): blocks of 256
+// threads with 16 items each, the sort tiles of the first pass.  Measured on
+// a B200 at 2^22 (c = 17, sort stage of the plain MSM, scan + first pass +
+// one look-back pass): 0.803 ms with these tiles, 0.822 with blocks of 512
+// threads x 12 items (tiles of 6144, 2 blocks per SM), 0.832 with the
+// earlier look-back over separate flag and count arrays.  (A standalone pass
+// over the same sizes favoured the larger tiles, 0.410 against 0.439 ms; in
+// the pipeline the gain did not hold.)
+constexpr unsigned LOOKBACK_THREADS = SORT_THREADS, LOOKBACK_ITEMS = SORT_ITEMS, LOOKBACK_TILE = LOOKBACK_THREADS * LOOKBACK_ITEMS;
+// Dynamic shared memory of a look-back tile of THREADS x ITEMS entries: the
+// staged tile (key and value in one 8-byte word) and per-warp digit counters.
+template <unsigned THREADS, unsigned ITEMS> constexpr size_t lookback_smem_bytes() {
+  return (size_t)THREADS * ITEMS * 8 + (size_t)(THREADS / 32) * SORT_RADIX * 4;
+}
 constexpr unsigned ACC_THREADS = 128;
 
 // Window w's entries start at w * window_stride(n): n rounded up to 32
@@ -80,6 +94,7 @@ struct plan {
   unsigned key_bits;    // bits of a sort key (|d| - 1 for |d| in [1, 2^log_b])
   unsigned sort_passes; // radix passes
   unsigned tiles;       // sort tiles per window
+  unsigned lookback_tiles; // look-back tiles (LOOKBACK_TILE entries) per window
   unsigned acc_threads; // accumulation threads (4 blocks of ACC_THREADS per SM at most)
   unsigned acc_ranges;  // accumulation ranges (>= acc_threads), handed out to warps
   unsigned log_m;       // log2 of the running-sum group
@@ -108,10 +123,12 @@ __global__ void digits_histogram_kernel(const fe *__restrict__ scalars, unsigned
                                         uint32_t *__restrict__ keys, uint32_t *__restrict__ vals, uint32_t *__restrict__ hist,
                                         uint32_t *__restrict__ totals, uint32_t *__restrict__ zeros);
 // a stable radix pass in one kernel, positions by decoupled look-back
+// (tiles: look-back tiles per window; words: [windows][tiles][256], zero at
+// launch; dynamic shared memory lookback_smem_bytes<LOOKBACK_THREADS,
+// LOOKBACK_ITEMS>())
 __global__ void lookback_stable_kernel(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in, uint32_t *__restrict__ keys_out,
-                                       uint32_t *__restrict__ vals_out, unsigned n, unsigned windows, unsigned tiles, unsigned shift, uint32_t *flags,
-                                       uint32_t *agg, uint32_t *incl, const uint32_t *__restrict__ totals, const uint32_t *__restrict__ zeros,
-                                       unsigned *tile_ctr, unsigned *error);
+                                       uint32_t *__restrict__ vals_out, unsigned n, unsigned windows, unsigned tiles, unsigned shift, uint32_t *words,
+                                       const uint32_t *__restrict__ totals, const uint32_t *__restrict__ zeros, unsigned *tile_ctr, unsigned *error);
 
 // ---------------------------------------------------------------------------
 // 2. sort (keys and values per window segment of n entries); the first pass

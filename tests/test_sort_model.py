@@ -4,21 +4,24 @@ sort_scatter_first_kernel, lookback_stable_kernel; tile code in
 msm_device.cuh): per-pass digit counts per tile from the digit kernel (the
 first pass's per tile, later passes' summed into digit totals), one scan
 giving the first pass's tile offsets and totals, the first pass (drops zero
-digits, any order among equal digits), then one kernel
-per later 8-bit pass in which each tile finds the positions of its digit runs
-by decoupled look-back: it publishes its aggregate, reads the flags of
-earlier tiles 32 at a time until it meets an inclusive count (waiting while a
-tile between has published nothing), adds that count and the aggregates after
-it, and publishes its inclusive count.  Tickets go to windows in turn and
-tiles finish in a random order.  Checked: the window segments come out
-grouped exactly by key (a stable sort of the first pass's output), at
-[w S + zeros_w, w S + n)."""
+digits, any order among equal digits), then one kernel per later 8-bit pass
+in which each tile finds, digit by digit, the positions of its runs by
+decoupled look-back over packed words (status in the top two bits, count
+below): it publishes its count as an aggregate, reads the earlier tiles' words
+of its digit eight at a time, newest first, adding counts until an inclusive
+one (waiting while a word is still empty), and publishes its inclusive count.
+The model gives the later passes a tile size of their own (the kernels may
+use one).  Tickets go to windows in turn and tiles and digits finish in a
+random order.  Checked: the window segments come out grouped exactly by key
+(a stable sort of the first pass's output), at [w S + zeros_w, w S + n)."""
 import random
 
 import pytest
 
-RADIX_BITS, RADIX, TILE = 8, 256, 64  # the model's tile is small so that windows span many tiles
-AGG, INCL = 1, 2
+RADIX_BITS, RADIX, TILE = 8, 256, 64  # the model's tiles are small so that windows span many tiles
+LOOKBACK_TILE = 96  # the later passes' tiles
+AGG, INCL, COUNT = 1 << 30, 2 << 30, (1 << 30) - 1  # look-back word: status bits over the count
+BATCH = 8
 ZERO_KEY = 0xFFFFFFFF
 
 
@@ -43,32 +46,33 @@ def model_sort(keys, vals, n, windows, stride, passes, rng):
     totals = [[[sum(hist[p][w][t][d] for t in range(tiles)) for d in range(RADIX)] for w in range(windows)] for p in range(passes)]
     # the scan: pass 0's exclusive prefix over tiles; later passes use look-back
     scan0 = [[[sum(hist[0][w][u][d] for u in range(t)) for d in range(RADIX)] for t in range(tiles)] for w in range(windows)]
-    flags = [[[0] * tiles for _ in range(windows)] for _ in range(passes)]
-    agg = [[[0] * RADIX for _ in range(tiles)] for _ in range(windows)]
-    incl = [[[0] * RADIX for _ in range(tiles)] for _ in range(windows)]
     cur_k, cur_v = list(keys), list(vals)
     for p in range(passes):
         shift = p * RADIX_BITS
+        size = TILE if p == 0 else LOOKBACK_TILE
+        ptiles = (n + size - 1) // size
+        words = [[[0] * RADIX for _ in range(ptiles)] for _ in range(windows)]  # cleared before the pass
         out_k, out_v = [None] * len(keys), [None] * len(vals)
         # every (window, tile) is one block; tickets go to windows in turn
         # (ticket = tile * windows + w) and blocks progress in a random order;
-        # a block's look-back only ever waits for earlier tiles of its window
-        pending = [(w, t) for t in range(tiles) for w in range(windows)]
+        # a block's look-back only ever waits for earlier tiles of its window,
+        # and each digit's look-back goes on by itself
+        pending = [(w, t) for t in range(ptiles) for w in range(windows)]
         rng.shuffle(pending)
-        published = set()
+        state = {}
         while pending:
             progressed = False
             for item in list(pending):
                 w, t = item
                 live = n if p == 0 else n - zeros[w]
-                base = t * TILE
+                base = t * size
                 if base >= live:
                     pending.remove(item)
                     progressed = True
                     continue
                 seg_in = w * stride if p == 0 else w * stride + zeros[w]
                 seg_out = w * stride + zeros[w]
-                items = [(cur_k[seg_in + base + i], cur_v[seg_in + base + i]) for i in range(min(TILE, live - base))]
+                items = [(cur_k[seg_in + base + i], cur_v[seg_in + base + i]) for i in range(min(size, live - base))]
                 if p == 0:
                     items = [it for it in items if it[0] != ZERO_KEY]
                     rng.shuffle(items)  # the first pass ranks equal digits in any order
@@ -78,27 +82,31 @@ def model_sort(keys, vals, n, windows, stride, passes, rng):
                 if p == 0:
                     prefix = scan0[w][t]
                 else:
-                    if item not in published:
-                        agg[w][t] = list(count)
-                        flags[p][w][t] = AGG
-                        published.add(item)
-                    # the first warp: flags of 32 earlier tiles at a time
-                    hi, start, blocked = t, -1, False
-                    while hi > 0:
-                        batch = [flags[p][w][hi - 1 - lane] if hi - 1 - lane >= 0 else AGG for lane in range(32)]
-                        nearest = next((lane for lane in range(32) if batch[lane] == INCL), 32)
-                        if any(batch[lane] == 0 for lane in range(nearest)):
-                            blocked = True
-                            break
-                        if nearest < 32:
-                            start = hi - 1 - nearest
-                            break
-                        hi -= 32
-                    if blocked:
-                        continue  # retry later, like the bounded poll
-                    prefix = [(incl[w][start][d] if start >= 0 else 0) + sum(agg[w][j][d] for j in range(start + 1, t)) for d in range(RADIX)]
-                    incl[w][t] = [prefix[d] + count[d] for d in range(RADIX)]
-                    flags[p][w][t] = INCL
+                    if item not in state:  # ranked: every digit publishes its count
+                        for d in range(RADIX):
+                            words[w][t][d] = (INCL if t == 0 else AGG) | count[d]
+                        state[item] = {"prefix": [0] * RADIX, "next": [t - 1] * RADIX, "done": [t == 0] * RADIX}
+                        progressed = True
+                    st = state[item]
+                    for d in rng.sample(range(RADIX), RADIX):  # digits in any order, one or two steps each
+                        for _ in range(rng.randint(1, 2)):
+                            if st["done"][d]:
+                                break
+                            j = st["next"][d]
+                            batch = [words[w][j - k][d] if j - k >= 0 else INCL for k in range(BATCH)]
+                            for v in batch:
+                                if v < AGG:
+                                    break  # empty: that tile has not ranked yet, poll again
+                                progressed = True
+                                st["prefix"][d] += v & COUNT
+                                st["next"][d] -= 1
+                                if v >= INCL:
+                                    st["done"][d] = True
+                                    words[w][t][d] = INCL | (st["prefix"][d] + count[d])
+                                    break
+                    if not all(st["done"]):
+                        continue
+                    prefix = st["prefix"]
                 dbase = [0] * RADIX
                 for d in range(1, RADIX):
                     dbase[d] = dbase[d - 1] + totals[p][w][d - 1]
