@@ -489,17 +489,34 @@ __device__ __forceinline__ uint2 scan2_256(uint32_t a, uint32_t b) {
   return make_uint2(ba + ia - a, bb + ib - b);
 }
 
-// One stable radix pass over one tile of `count` entries (at most THREADS *
-// ITEMS) at seg + base, base = tile * THREADS * ITEMS, written to the same
-// segment of the output arrays.  Ranks among equal digits warp by warp, 32
-// consecutive items per round (warp_peers), then per digit: the prefix over
-// warps, the tile's count published and the count over earlier tiles found
-// by look-back (lookback_digit; the first 256 threads, one digit each), the
-// digit's run position = its total over smaller digits (totals: the
-// segment's digit totals) + that prefix.  The tile is then reordered in
-// shared memory so that each digit's run is written with consecutive
-// addresses.  Needs lookback_smem_bytes<THREADS, ITEMS>() of dynamic shared
-// memory.
+// Tiles of a later pass whose entries span at most LOOKBACK_SEGMENTS values
+// of the key bits below `shift` rank with shared atomics per (value, digit)
+// instead of ballots (see lookback_tile).
+constexpr unsigned LOOKBACK_SEGMENTS = 4;
+
+// One radix pass after the first over one tile of `count` entries (at most
+// THREADS * ITEMS) at seg + base, base = tile * THREADS * ITEMS, written to
+// the same segment of the output arrays, so that the segment ends up sorted
+// by the key bits up to shift + 8.  The input is sorted by the bits below
+// `shift` (the earlier passes), so equal digits must keep the order of those
+// bits; entries with equal keys up to shift + 8 may take any order (they
+// fall into one bucket).  Ranking among equal digits:
+//  * when the tile's entries span at most LOOKBACK_SEGMENTS values v of the
+//    lower bits (known from its first and last entry, as the tile is sorted
+//    by them; the common case for large windows, where a value's entries
+//    fill many tiles), with shared atomics on a counter per (v - first value,
+//    digit): the digit's run in the tile holds segment 0's entries, then
+//    segment 1's, ... — what a stable pass would give, up to the order of
+//    equal keys;
+//  * otherwise stably, warp by warp, 32 consecutive items per round
+//    (warp_peers), with a counter per (warp, digit).
+// Then per digit: the prefix over the counter rows, the tile's count
+// published and the count over earlier tiles found by look-back
+// (lookback_digit; the first 256 threads, one digit each), the digit's run
+// position = its total over smaller digits (totals: the segment's digit
+// totals) + that prefix.  The tile is then reordered in shared memory so
+// that each digit's run is written with consecutive addresses.  Needs
+// lookback_smem_bytes<THREADS, ITEMS>() of dynamic shared memory.
 template <unsigned THREADS, unsigned ITEMS>
 __device__ __forceinline__ void lookback_tile(const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in,
                                               uint32_t *__restrict__ keys_out, uint32_t *__restrict__ vals_out, size_t seg, unsigned tile,
@@ -507,47 +524,64 @@ __device__ __forceinline__ void lookback_tile(const uint32_t *__restrict__ keys_
                                               unsigned *error) {
   constexpr unsigned TILE = THREADS * ITEMS, WARPS = THREADS / 32;
   static_assert(THREADS >= SORT_RADIX && THREADS % 32 == 0, "look-back tile: at least one thread per digit");
+  static_assert(LOOKBACK_SEGMENTS <= WARPS, "segment counters share the per-warp counter rows");
   extern __shared__ uint2 lookback_shared[];
   uint2 *s_kv = lookback_shared;
-  uint32_t(*whist)[SORT_RADIX] = reinterpret_cast<uint32_t(*)[SORT_RADIX]>(lookback_shared + TILE);
+  // counter rows: per warp (stable ranking) or per segment (atomic ranking)
+  uint32_t(*rows)[SORT_RADIX] = reinterpret_cast<uint32_t(*)[SORT_RADIX]>(lookback_shared + TILE);
   __shared__ uint32_t tile_off[SORT_RADIX], delta[SORT_RADIX];
   __shared__ uint32_t staged;
   const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const unsigned sub = warp * (32 * ITEMS); // this warp's items: base + sub + r*32 + lane
   const size_t base = (size_t)tile * TILE;
   for (unsigned d = lane; d < SORT_RADIX; d += 32)
-    whist[warp][d] = 0;
-  __syncthreads();
+    rows[warp][d] = 0;
   uint32_t key[ITEMS], val[ITEMS], rank[ITEMS];
-  const unsigned lt_mask = (1u << lane) - 1;
-  // every item's loads first, so that all of them are in flight together
+  // every item's loads first, so that all of them are in flight together;
+  // the tile's first and last key give the span of its lower bits
+  const uint32_t lower_mask = (1u << shift) - 1;
+  const uint32_t first_lower = keys_in[seg + base] & lower_mask, last_lower = keys_in[seg + base + count - 1] & lower_mask;
 #pragma unroll
   for (unsigned r = 0; r < ITEMS; r++) {
     const unsigned i = sub + r * 32 + lane;
     key[r] = i < count ? keys_in[seg + base + i] : 0;
     val[r] = i < count ? vals_in[seg + base + i] : 0;
   }
+  const bool segmented = last_lower - first_lower < LOOKBACK_SEGMENTS; // the same in every thread
+  __syncthreads();
+  // the counter row of an item: its segment (clamped, so that input that is
+  // not sorted as it should be still stays inside the tile) or its warp
+  auto row_of = [&](uint32_t k) { return segmented ? min((k & lower_mask) - first_lower, LOOKBACK_SEGMENTS - 1) : warp; };
+  if (segmented) {
 #pragma unroll
-  for (unsigned r = 0; r < ITEMS; r++) {
-    const unsigned i = sub + r * 32 + lane;
-    const bool valid = i < count;
-    const unsigned d = valid ? sort_digit(key[r], shift) : SORT_RADIX;
-    const unsigned peers = warp_peers(d);
-    const uint32_t before = valid ? whist[warp][d] : 0;
-    __syncwarp();
-    if (valid && lane == (unsigned)(__ffs(peers) - 1))
-      whist[warp][d] = before + __popc(peers);
-    __syncwarp();
-    rank[r] = before + __popc(peers & lt_mask);
+    for (unsigned r = 0; r < ITEMS; r++) {
+      const unsigned i = sub + r * 32 + lane;
+      rank[r] = i < count ? atomicAdd(&rows[row_of(key[r])][sort_digit(key[r], shift)], 1u) : 0;
+    }
+  } else {
+    const unsigned lt_mask = (1u << lane) - 1;
+#pragma unroll
+    for (unsigned r = 0; r < ITEMS; r++) {
+      const unsigned i = sub + r * 32 + lane;
+      const bool valid = i < count;
+      const unsigned d = valid ? sort_digit(key[r], shift) : SORT_RADIX;
+      const unsigned peers = warp_peers(d);
+      const uint32_t before = valid ? rows[warp][d] : 0;
+      __syncwarp();
+      if (valid && lane == (unsigned)(__ffs(peers) - 1))
+        rows[warp][d] = before + __popc(peers);
+      __syncwarp();
+      rank[r] = before + __popc(peers & lt_mask);
+    }
   }
   __syncthreads();
   uint32_t own = 0, prefix = 0, total = 0;
   if (threadIdx.x < SORT_RADIX) {
     const unsigned d = threadIdx.x;
 #pragma unroll
-    for (unsigned k = 0; k < WARPS; k++) { // per digit: exclusive prefix over warps (warp order = item order)
-      const uint32_t t = whist[k][d];
-      whist[k][d] = own;
+    for (unsigned k = 0; k < WARPS; k++) { // per digit: exclusive prefix over the rows (row order = item order)
+      const uint32_t t = rows[k][d];
+      rows[k][d] = own;
       own += t;
     }
     prefix = lookback_digit(words, tile, d, own, error);
@@ -566,7 +600,7 @@ __device__ __forceinline__ void lookback_tile(const uint32_t *__restrict__ keys_
     const unsigned i = sub + r * 32 + lane;
     if (i < count) {
       const unsigned d = sort_digit(key[r], shift);
-      s_kv[tile_off[d] + whist[warp][d] + rank[r]] = make_uint2(key[r], val[r]);
+      s_kv[tile_off[d] + rows[row_of(key[r])][d] + rank[r]] = make_uint2(key[r], val[r]);
     }
   }
   __syncthreads();
