@@ -491,8 +491,9 @@ __device__ __forceinline__ uint2 scan2_256(uint32_t a, uint32_t b) {
 
 // Tiles of a later pass whose entries span at most LOOKBACK_SEGMENTS values
 // of the key bits below `shift` rank with shared atomics per (value, digit)
-// instead of ballots (see lookback_tile).
-constexpr unsigned LOOKBACK_SEGMENTS = 4;
+// instead of ballots (see lookback_tile); one counter row per value, in the
+// rows the ballot ranking keeps per warp.
+constexpr unsigned LOOKBACK_SEGMENTS = 8;
 
 // One radix pass after the first over one tile of `count` entries (at most
 // THREADS * ITEMS) at seg + base, base = tile * THREADS * ITEMS, written to

@@ -10,7 +10,7 @@ decoupled look-back over packed words (status in the top two bits, count
 below): it publishes its count as an aggregate, reads the earlier tiles' words
 of its digit eight at a time, newest first, adding counts until an inclusive
 one (waiting while a word is still empty), and publishes its inclusive count.
-A later-pass tile whose entries span at most four values of the lower key
+A later-pass tile whose entries span at most eight values of the lower key
 bits ranks equal digits in any order within each value (the kernels' atomic
 ranking), others stably.  The model gives the later passes a tile size of
 their own (the kernels may use one).  Tickets go to windows in turn and tiles and digits finish in a
@@ -24,7 +24,7 @@ RADIX_BITS, RADIX, TILE = 8, 256, 64  # the model's tiles are small so that wind
 LOOKBACK_TILE = 96  # the later passes' tiles
 AGG, INCL, COUNT = 1 << 30, 2 << 30, (1 << 30) - 1  # look-back word: status bits over the count
 BATCH = 8
-SEGMENTS = 4  # lower-bit values a later-pass tile may span and still rank with atomics
+SEGMENTS = 8  # lower-bit values a later-pass tile may span and still rank with atomics
 ZERO_KEY = 0xFFFFFFFF
 
 
@@ -150,7 +150,7 @@ def test_onesweep_model_sorts_each_window(trial):
             r = rng.random()
             k = ZERO_KEY if r < zero_share else (hot if r < zero_share + 0.2 else rng.randrange(1 << key_bits))
             if trial >= 6 and k != ZERO_KEY:  # few distinct low bytes: later-pass tiles span few values
-                k = (k & ~0xFF) | rng.choice([3, 4, 9])
+                k = (k & ~0xFF) | rng.choice([3, 4, 9, 30])
             keys[w * stride + i] = k
             vals[w * stride + i] = i | (rng.randrange(2) << 31)
     out_k, out_v, zeros = model_sort(keys, vals, n, windows, stride, passes, rng)
