@@ -336,6 +336,70 @@ def test_sort_tile_edges(gpu, oracle, n, window_bits):
     assert oracle.horner(res) == oracle.msm_checksum(k, scalars)
 
 
+def crafted_window_scalars(n: int, seed: int):
+    """Scalars with chosen 16-bit signed digits, one sort-key pattern per
+    window (window w of width 16 holds bits [16 w, 16 w + 16); every digit
+    lies in [0, 2^15], so the recoding takes it as is, and the top digit
+    stays below 2^11, so s < r / 2 and the fold keeps s).  Windows cycle
+    through four patterns of the key |d| - 1: uniform; low byte 5 or 12;
+    low byte 5 or 13; 95 % zero digits and uniform otherwise.  Returns
+    (Montgomery scalars, the (16, n) digit matrix)."""
+    g = np.random.Generator(np.random.PCG64(np.random.SeedSequence([seed, 9])))
+    digits = np.zeros((16, n), np.int64)
+    for w in range(16):
+        mode = w % 4
+        if mode == 0:
+            d = g.integers(1, (1 << 15) + 1, n)
+        elif mode in (1, 2):
+            low = np.where(g.integers(0, 2, n) == 0, 5, 12 if mode == 1 else 13)
+            d = ((g.integers(0, 1 << 7, n) << 8) | low) + 1
+        else:
+            d = np.where(g.random(n) < 0.95, 0, g.integers(1, (1 << 15) + 1, n))
+        if w == 15:
+            d = np.minimum(d, 1 << 11)
+        digits[w] = d
+    limbs = np.zeros((n, 8), np.uint64)
+    for w in range(16):
+        limbs[:, w // 2] |= digits[w].astype(np.uint64) << np.uint64(16 * (w % 2))
+    mont = np.empty((n, 8), np.uint32)
+    for i in range(n):
+        v = int.from_bytes(limbs[i].astype(np.uint32).tobytes(), "little")
+        assert 2 * v < synth.R
+        mont[i] = np.frombuffer(((v * synth.MONT_R) % synth.R).to_bytes(32, "little"), np.uint32)
+    return mont, digits
+
+
+def test_lookback_ranking_paths(gpu, oracle):
+    """The second radix pass ranks a tile with shared atomics when its keys'
+    low bytes span fewer than eight values and with ballots otherwise.  At
+    n = 2^19 + 4099 and 16-bit windows (two passes, look-back tiles of 4096
+    keys over each window's nonzero entries, sorted by the low byte by the
+    first pass) the crafted windows give tiles spanning 1-3 values (uniform
+    keys), exactly 7 (low bytes 5 and 12: the atomic path's last counter
+    row), exactly 8 (5 and 13: ballots) and dozens (sparse windows: ballots).
+    The spans are checked on the host first; the MSM must equal the checksum
+    oracle."""
+    n = (1 << 19) + 4099
+    scalars, digits = crafted_window_scalars(n, 41)
+    spans = set()
+    for w in range(16):
+        keys = np.sort((digits[w][digits[w] > 0] - 1) & 0xFF, kind="stable")
+        for t in range(0, len(keys), 4096):
+            tile = keys[t:t + 4096]
+            spans.add(int(tile[-1] - tile[0]))
+    assert {0, 7, 8}.issubset(spans) and max(spans) > 8
+    k = synth.base_multipliers(41, n)
+    bd, _ = generated_bases(gpu, k)
+    sd = gpu.upload(scalars)
+    rd = gpu.bc.malloc(254 * 96)
+    assert gpu.bc.msm_any(gpu.pool, gpu.stream, bd, sd, rd, n, 16) == 0
+    gpu.bc.stream_synchronize(gpu.stream)
+    res = gpu.bc.from_device(rd, (254, 24))
+    for p in (bd, sd, rd):
+        gpu.bc.free(p)
+    assert oracle.horner(res) == oracle.msm_checksum(k, scalars)
+
+
 @pytest.mark.parametrize("dist", ["uniform", "skewed"])
 def test_full_size_2_22(gpu, oracle, dist):
     """Configs 1 and 2 (N = 2^22, seeds 1 and 2) against the checksum oracle."""
