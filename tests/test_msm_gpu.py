@@ -322,8 +322,11 @@ def test_any_window_and_length(gpu, oracle, window_bits):
 def test_sort_tile_edges(gpu, oracle, n, window_bits):
     """Lengths just past and short of whole sort tiles (4096 keys), skewed
     scalars (many zero digits, one heavy bucket): the first pass's partial last
-    tile and the look-back passes over windows whose nonzero entries start
-    mid-tile; 9-bit windows take one radix pass, the others two."""
+    tile and the later passes over windows whose nonzero entries start
+    mid-tile; 9-bit windows take one radix pass, the others two.  Below 128
+    sort tiles these run the histogram + scan + scatter passes; the look-back
+    passes over such windows are covered by test_lookback_ranking_paths and
+    the tests from 2^19 points up."""
     scalars, k = synth.workload("skewed", n, 500 + n % 97)
     bd, _ = generated_bases(gpu, k)
     sd = gpu.upload(scalars)
